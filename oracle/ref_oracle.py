@@ -1,0 +1,162 @@
+"""ctypes driver for the compiled reference solver (oracle/_ref/libhfps_ref.so).
+
+Test infrastructure only (tests/, smoke() and bench.py's CPU legs): it runs
+the reference's own NativeCartesianMgPlan, solve_pcg and solve_fgmres on a
+PressureSystem.  Build it with ``make -C oracle ref`` in a tree where the
+reference sources exist; the built library then travels with the checkout.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY = os.path.join(HERE, "_ref", "libhfps_ref.so")
+
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIBRARY)
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        lib = ctypes.CDLL(LIBRARY)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        lib.hfref_create.argtypes = [ctypes.c_int] * 3 + [dp] * 3 + [ip] + [dp] * 4 + [
+            ctypes.c_void_p, ip, dp, ctypes.POINTER(ctypes.c_void_p)]
+        lib.hfref_create.restype = ctypes.c_int
+        lib.hfref_destroy.argtypes = [ctypes.c_void_p]
+        lib.hfref_levels.argtypes = [ctypes.c_void_p, ip, ctypes.c_int]
+        lib.hfref_levels.restype = ctypes.c_int
+        lib.hfref_apply_operator.argtypes = [ctypes.c_void_p, dp, dp]
+        lib.hfref_apply_mg.argtypes = [ctypes.c_void_p, dp, dp]
+        lib.hfref_solve.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, dp]
+        _lib = lib
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@dataclasses.dataclass
+class MgPolicy:
+    """MgHierarchyPolicy fields (include/hundun/v04_linear.hpp:115-131).
+
+    Defaults are the struct defaults: red-black V(2,2), 24 coarse sweeps.
+    ``production()`` is production_pressure_mg_policy
+    (src/solver_piso_detail.hpp:10-19).
+    """
+
+    smoother: int = 0  # 0 red-black, 1 Chebyshev-Jacobi
+    cycle: int = 0  # 0 V, 1 F
+    pre: int = 2
+    post: int = 2
+    coarse_sweeps: int = 24
+    max_levels: int = 32
+    min_coarse_extent: int = 3
+    chebyshev_fraction: float = 0.3
+    anisotropy_threshold: float = 4.0
+    diagonal_shortcut: float = 0.0
+
+    @staticmethod
+    def production() -> "MgPolicy":
+        return MgPolicy(smoother=1, cycle=1, pre=1, post=2, diagonal_shortcut=0.1)
+
+
+class RefSession:
+    """One compiled reference plan (geometry + coefficients + MG hierarchy)."""
+
+    TERMINATION = ["converged", "zero_rhs", "maximum_iterations", "breakdown", "non_finite",
+                   "operator_failure", "preconditioner_failure", "collective_failure",
+                   "invalid_plan", "convergence_audit_failure"]
+
+    def __init__(self, system, policy: Optional[MgPolicy] = None, algorithm: str = "pcg",
+                 restart: int = 12, unit_linear: Optional[bool] = None):
+        lib = _load()
+        self.system = system
+        policy = policy or MgPolicy()
+        if unit_linear is None:
+            unit_linear = algorithm == "pcg"
+        nx, ny, nz = system.shape
+        self._faces = [np.ascontiguousarray(f, dtype=np.float64) for f in system.faces]
+        self._bc = (ctypes.c_int * 6)(*system.boundary)
+        options = (ctypes.c_int * 10)(1 if algorithm == "fgmres" else 0, restart, policy.smoother,
+                                      policy.cycle, policy.pre, policy.post, policy.coarse_sweeps,
+                                      1 if unit_linear else 0, policy.max_levels,
+                                      policy.min_coarse_extent)
+        reals = (ctypes.c_double * 3)(policy.chebyshev_fraction, policy.anisotropy_threshold,
+                                      policy.diagonal_shortcut)
+        active = None
+        if system.active is not None:
+            self._active = np.ascontiguousarray(system.active, dtype=np.uint8)
+            active = self._active.ctypes.data_as(ctypes.c_void_p)
+        handle = ctypes.c_void_p()
+        rc = lib.hfref_create(nx, ny, nz, _dp(self._faces[0]), _dp(self._faces[1]),
+                              _dp(self._faces[2]), self._bc, _dp(system.diagonal),
+                              _dp(system.face_x), _dp(system.face_y), _dp(system.face_z), active,
+                              options, reals, ctypes.byref(handle))
+        if rc != 0:
+            raise RuntimeError(f"reference plan compile failed: status {rc}")
+        self._handle = handle
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.hfref_destroy(self._handle)
+            self._handle = None
+
+    __del__ = close
+
+    def levels(self):
+        shapes = (ctypes.c_int * 128)()
+        count = self._lib.hfref_levels(self._handle, shapes, 32)
+        return [tuple(shapes[4 * i:4 * i + 4]) for i in range(count)]
+
+    def apply_operator(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        rc = self._lib.hfref_apply_operator(self._handle, _dp(x), _dp(y))
+        if rc != 0:
+            raise RuntimeError(f"reference operator failed: {rc}")
+        return y
+
+    def apply_mg(self, r: np.ndarray) -> np.ndarray:
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty_like(r)
+        rc = self._lib.hfref_apply_mg(self._handle, _dp(r), _dp(z))
+        if rc != 0:
+            raise RuntimeError(f"reference MG apply failed: {rc}")
+        return z
+
+    def solve(self, rhs: np.ndarray, x0: Optional[np.ndarray] = None, rtol: float = 1e-10,
+              atol: float = 0.0, maxit: int = 400, true_residual_interval: int = 4):
+        rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+        x = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64, order="C")
+        out = np.zeros(10)
+        rc = self._lib.hfref_solve(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
+                                   true_residual_interval, _dp(out))
+        info = {
+            "status": rc,
+            "iterations": int(out[0]),
+            "initial_true_residual": out[1],
+            "final_true_residual": out[2],
+            "termination": self.TERMINATION[int(out[3])] if 0 <= out[3] < 10 else int(out[3]),
+            "rhs_norm": out[4],
+            "limit": out[5],
+            "operator_applies": int(out[6]),
+            "preconditioner_applies": int(out[7]),
+            "seconds": out[8],
+            "setup_seconds": out[9],
+        }
+        return x, info
