@@ -1,0 +1,391 @@
+"""Benchmark of the B200 pressure solve (one JSON line on rank 0).
+
+Workload: the 256^3 pressure system with geometric y-stretching (ratio 1.02
+toward y=0), a wrinkled flame density front (rho ratio 7) and a solid IBM
+z-cylinder, Dirichlet p=0 on x-max and Neumann elsewhere, solved to 1e-10
+relative FP64 true residual by MG-preconditioned CG (the reference's
+solve_pcg control flow, true residual every 4 iterations) with the
+reference's production MG policy (F-cycle, pre 1 / post 2 sweeps; the
+y-strong grid selects y-line relaxation and x/z semicoarsening).  A step is
+one solve of the PISO-like warm-start sequence: rhs_k = rhs_0 + 0.05 * div
+(fresh N(0,1) face noise, seed k), x0 = previous solution.  Inputs are
+seeded synthetic fields (no public dataset exists for this path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun): the
+solve of one system does not shard across GPUs in this build.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "hundun-flow_b200"))
+
+METRIC = "time to 1e-10 rel. residual at 256³, mixed vs FP64 MG-PCG; solves/s; HBM GB/s"
+UNIT = "solves/s"
+CONFIG_NAME = "wrinkled256"
+RTOL = 1e-10
+TRUE_RESIDUAL_INTERVAL = 4
+WARM_SEQUENCE = 20
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--shape", type=int, nargs=3, default=None,
+                   help="override the grid (testing only; the bench line is the 256^3 case)")
+    p.add_argument("--single", choices=["fp64", "mixed"], default=None,
+                   help="profiling aid: one warm-up solve, then one solve, no timing/JSON")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, value):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_system(args):
+    from hfps import workloads
+    kw = {}
+    if args.shape:
+        kw["n"] = tuple(args.shape)
+    return workloads.make(CONFIG_NAME, **kw)
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        self.file.seek(0)
+        mhz, max_mhz, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1]))
+                max_mhz.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        if not mhz:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": max(max_mhz),
+                "reasons": sorted(reasons), "samples": len(mhz)}
+
+
+class ReferenceSampler:
+    """The reference's own solve_pcg + NativeCartesianMgPlan (compiled from
+    the reference sources into oracle/_ref) on the full system, timed for a
+    bounded number of PCG iterations per sample; the C restatement stands in
+    when the compiled reference is absent."""
+
+    def __init__(self, system):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ref_oracle
+        self.system = system
+        if ref_oracle.available():
+            self.session = ref_oracle.RefSession(system, ref_oracle.MgPolicy.production(),
+                                                 algorithm="pcg")
+            self.kind = "reference"
+        else:
+            import c_oracle
+            self.session = c_oracle.OracleSession(system, ref_oracle.MgPolicy.production())
+            self.kind = "port"
+
+    def seconds_per_iteration(self, iterations: int = 1) -> float:
+        t0 = time.perf_counter()
+        _, info = self.session.solve(self.system.rhs, None, rtol=RTOL, maxit=iterations,
+                                     true_residual_interval=TRUE_RESIDUAL_INTERVAL)
+        return (time.perf_counter() - t0) / max(1, info["iterations"])
+
+    def close(self):
+        self.session.close()
+
+
+def run_reference(args, world, rank):
+    """The reference arm: the reference's own CPU MG-PCG on this workload."""
+    if rank != 0:
+        return
+    system = make_system(args)
+    sampler = ReferenceSampler(system)
+    kind = sampler.kind
+    per_iteration = []
+    for step in range(args.warmup + args.steps):
+        seconds = sampler.seconds_per_iteration(1)
+        if step >= args.warmup:
+            per_iteration.append(seconds)
+    sampler.close()
+    t_iter = statistics.mean(per_iteration)
+    iterations = REFERENCE_ITERATIONS_PER_SOLVE
+    value = 1.0 / (t_iter * iterations)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64/Box-Muller)",
+        "config": {"workload": "wrinkled256 warm-start pressure solve", "shape": list(system.shape),
+                   "algorithm": "solve_pcg + NativeCartesianMgPlan (production policy, unit_linear)",
+                   "rtol": RTOL},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
+                         "sample": f"{args.steps} x 1 PCG iteration of the 256^3 system "
+                                   f"({t_iter:.2f} s each) x {iterations} iterations per solve"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# Iterations the reference solve_pcg (production MG, unit_linear) needs per
+# warm-started solve of this workload: 41, 41, 41 for steps 1-3, measured by
+# running the compiled reference to convergence on the same inputs (the cold
+# first solve takes 53).
+REFERENCE_ITERATIONS_PER_SOLVE = 41
+
+
+def run_b200(args, world, rank, local):
+    import numpy as np
+    import torch
+    import hfps
+    from hfps import workloads
+
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    system = make_system(args)
+    stream = torch.cuda.current_stream(device)
+    solver = hfps.PressureSolver.from_system(system, hfps.Policy.production(), stream=stream)
+    n = system.cells
+    rhs0 = torch.from_numpy(system.rhs.reshape(-1)).to(device)
+    total = args.warmup + args.steps
+    rhs = []
+    for k in range(total):
+        seed = 1 + (k % WARM_SEQUENCE)
+        rhs.append(rhs0 + workloads.flux_divergence_rhs_torch(
+            seed, system.faces, system.boundary, system.active, 0.05, device=device))
+    opts = hfps.SolveOptions(rtol=RTOL, maxit=400, true_residual_interval=TRUE_RESIDUAL_INTERVAL)
+    x = torch.zeros(n, dtype=torch.float64, device=device)
+
+    def run_sequence(precision, steps, xbuf, offset=0, record=None):
+        o = hfps.SolveOptions(rtol=RTOL, maxit=400, true_residual_interval=TRUE_RESIDUAL_INTERVAL,
+                              precision=precision)
+        for k in range(steps):
+            _, info = solver.solve(rhs[(offset + k) % total], x0=xbuf, out=xbuf, options=o,
+                                   history=False)
+            if record is not None:
+                record.append(info)
+
+    # Warm-up (also instantiates the MG graphs).
+    run_sequence(hfps.FP64, args.warmup, x)
+    xw = x.clone()
+    infos = []
+    barrier(world)
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        run_sequence(hfps.FP64, args.steps, x, offset=args.warmup, record=infos)
+        stop.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    seconds = max_over_ranks(world, start.elapsed_time(stop) / 1000.0)
+    value = world * args.steps / seconds
+
+    # Mixed precision on the same sequence (same warm-start state).
+    xm = xw.clone()
+    run_sequence(hfps.MIXED, 1, xm.clone(), offset=args.warmup)
+    minfos = []
+    torch.cuda.synchronize()
+    start.record(stream)
+    run_sequence(hfps.MIXED, args.steps, xm, offset=args.warmup, record=minfos)
+    stop.record(stream)
+    torch.cuda.synchronize()
+    mixed_seconds = max_over_ranks(world, start.elapsed_time(stop) / 1000.0)
+    mixed_error = float(torch.linalg.vector_norm(xm - x) / torch.linalg.vector_norm(x))
+
+    # End to end through the C ABI with pinned host buffers: every step copies
+    # rhs and x0 host->device and x device->host.
+    host_rhs = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in range(args.steps)]
+    for k in range(args.steps):
+        host_rhs[k].copy_(rhs[args.warmup + k])
+    host_x = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    host_x.copy_(xw)
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        solver.solve(host_rhs[k], x0=host_x, out=host_x, options=opts, history=False)
+    torch.cuda.synchronize()
+    e2e_seconds = max_over_ranks(world, time.perf_counter() - t0)
+    e2e_value = world * args.steps / e2e_seconds
+
+    # Dominant kernel: the level-0 line-relaxation colour pass (largest share
+    # of device time in the launch list).  Timed with CUDA events on the
+    # solver's stream; algorithmic bytes = 28 B per level-0 cell per pass.
+    kernels = {}
+    for name in ("smooth_fp64", "operator", "restrict_fp64", "prolong_fp64", "pcg_update",
+                 "smooth_fp32", "mg_fp64", "mg_mixed"):
+        ms, nbytes = solver.profile_kernel(name, 10)
+        kernels[name] = {"ms": ms, "bytes": nbytes,
+                         "gbs": (nbytes / (ms * 1e-3) / 1e9) if nbytes > 0 else None}
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        with open(peaks_path) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+        peak_note = "measured"
+    else:
+        peak, peak_note = 6650.0, "fallback"
+    dom = kernels["smooth_fp64"]
+    roofline = {"bound": "hbm", "kernel": "k_line_color<double> level 0 (one zebra colour)",
+                "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": dom["gbs"] / peak, "peak_source": peak_note,
+                "traffic": None, "bytes_per_launch": dom["bytes"], "ms_per_launch": dom["ms"]}
+
+    iterations = [i["iterations"] for i in infos]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sampler = ReferenceSampler(system)
+        kind = sampler.kind
+        t_iter = sampler.seconds_per_iteration(2)
+        sampler.close()
+        cpu = {"value": 1.0 / (t_iter * REFERENCE_ITERATIONS_PER_SOLVE), "unit": UNIT, "cores": 1,
+               "kind": kind,
+               "sample": f"2 PCG iterations of the 256^3 system ({t_iter:.2f} s each) x "
+                         f"{REFERENCE_ITERATIONS_PER_SOLVE} iterations per solve"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * seconds / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded SplitMix64/Box-Muller face-flux divergence)",
+            "config": {"workload": "wrinkled256 warm-start pressure solve (configs[1])",
+                       "shape": list(system.shape), "stretch_y": 1.02,
+                       "algorithm": "PCG (solve_pcg control flow) + MG production policy, unit_linear",
+                       "rtol": RTOL, "true_residual_interval": TRUE_RESIDUAL_INTERVAL,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (FP64 hierarchy ~2 GB per GPU)",
+                       "iterations_per_solve": iterations},
+            "mixed": {"value": world * args.steps / mixed_seconds, "unit": UNIT,
+                      "speedup_vs_fp64": seconds / mixed_seconds,
+                      "iterations_per_solve": [i["iterations"] for i in minfos],
+                      "rel_error_vs_fp64": mixed_error},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * n * 8,
+                    "d2h_bytes_per_step": n * 8},
+            "roofline": roofline,
+            "kernels": kernels,
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": int(sum(i["kernel_launches"] for i in infos)),
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+
+
+def run_single(args):
+    """One warm-up solve and one measured-by-profiler solve of step 1."""
+    import torch
+    import hfps
+    from hfps import workloads
+    system = make_system(args)
+    solver = hfps.PressureSolver.from_system(system, hfps.Policy.production(),
+                                             stream=torch.cuda.current_stream())
+    rhs = torch.from_numpy(system.rhs.reshape(-1)).cuda()
+    rhs1 = rhs + workloads.flux_divergence_rhs_torch(1, system.faces, system.boundary,
+                                                     system.active, 0.05)
+    precision = hfps.MIXED if args.single == "mixed" else hfps.FP64
+    opts = hfps.SolveOptions(rtol=RTOL, maxit=400, true_residual_interval=TRUE_RESIDUAL_INTERVAL,
+                             precision=precision)
+    x, info0 = solver.solve(rhs, options=opts, history=False)
+    x, info1 = solver.solve(rhs1, x0=x, out=x, options=opts, history=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"single": args.single, "iterations": [info0["iterations"], info1["iterations"]],
+                      "kernel_launches": [info0["kernel_launches"], info1["kernel_launches"]]}))
+    solver.close()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.single:
+        run_single(args)
+        return
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_b200(args, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

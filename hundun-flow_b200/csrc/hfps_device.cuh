@@ -1,0 +1,163 @@
+// Device-side building blocks of the B200 pressure solve.
+//
+// Layout (shared with the host and the C ABI): cell fields are dense and
+// x-fastest; x/y/z face arrays have extents (nx+1,ny,nz), (nx,ny+1,nz),
+// (nx,ny,nz+1).  For a cell c = i + nx*(j + ny*k) the six faces are
+//   x: c + j + ny*k  and +1        y: c + nx*k  and +nx
+//   z: c             and +nx*ny
+// so every kernel addresses faces from the cell index with two adds.
+//
+// The library is compiled with --fmad=false: the 7-point row is evaluated
+// as separate IEEE multiplies and subtractions in the reference's order
+// (point_row_value, src/solver_mg.cpp:2395-2414), which makes the level
+// operators, smoothers and transfers bit-identical to the reference's.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hfps {
+
+// Bit f of `neumann` is set when face f (x-,x+,y-,y+,z-,z+) is Neumann; a
+// clear bit is Dirichlet (neighbour value 0).  Neumann reads the cell
+// itself (MgPointBoundaryMode::self, src/solver_mg.cpp:940-963).
+template <class T>
+struct Level {
+  int nx, ny, nz;
+  unsigned neumann;
+  const T* __restrict__ diag;
+  const T* __restrict__ fx;
+  const T* __restrict__ fy;
+  const T* __restrict__ fz;
+  const uint8_t* __restrict__ fluid;  // 1 where the fluid volume is > 0
+};
+
+struct Index3 {
+  int i, j, k;
+  int c;
+};
+
+template <class T>
+__device__ __forceinline__ int face_x_index(const Level<T>& L, int c, int j,
+                                            int k) {
+  return c + j + L.ny * k;
+}
+template <class T>
+__device__ __forceinline__ int face_y_index(const Level<T>& L, int c, int k) {
+  return c + L.nx * k;
+}
+
+// A x at one cell, in the reference's accumulation order.
+template <class T>
+__device__ __forceinline__ T row_value(const Level<T>& L,
+                                       const T* __restrict__ x, int i, int j,
+                                       int k, int c) {
+  const int plane = L.nx * L.ny;
+  const T xc = x[c];
+  const T xm = i > 0 ? x[c - 1] : ((L.neumann & 1u) ? xc : T(0));
+  const T xp = i + 1 < L.nx ? x[c + 1] : ((L.neumann & 2u) ? xc : T(0));
+  const T ym = j > 0 ? x[c - L.nx] : ((L.neumann & 4u) ? xc : T(0));
+  const T yp = j + 1 < L.ny ? x[c + L.nx] : ((L.neumann & 8u) ? xc : T(0));
+  const T zm = k > 0 ? x[c - plane] : ((L.neumann & 16u) ? xc : T(0));
+  const T zp = k + 1 < L.nz ? x[c + plane] : ((L.neumann & 32u) ? xc : T(0));
+  const int fxi = face_x_index(L, c, j, k);
+  const int fyi = face_y_index(L, c, k);
+  T v = L.diag[c] * xc;
+  v -= L.fx[fxi] * xm;
+  v -= L.fx[fxi + 1] * xp;
+  v -= L.fy[fyi] * ym;
+  v -= L.fy[fyi + L.nx] * yp;
+  v -= L.fz[c] * zm;
+  v -= L.fz[c + plane] * zp;
+  return v;
+}
+
+// Neighbour along `axis` in direction `dir` for the line smoother's
+// transverse and end terms (level_neighbor, src/solver_mg.cpp:2222-2262).
+template <class T>
+__device__ __forceinline__ T line_neighbour(const Level<T>& L,
+                                            const T* __restrict__ x, int i,
+                                            int j, int k, int c, int axis,
+                                            int dir) {
+  if (axis == 0) {
+    if (dir < 0) return i > 0 ? x[c - 1] : ((L.neumann & 1u) ? x[c] : T(0));
+    return i + 1 < L.nx ? x[c + 1] : ((L.neumann & 2u) ? x[c] : T(0));
+  }
+  if (axis == 1) {
+    if (dir < 0) return j > 0 ? x[c - L.nx] : ((L.neumann & 4u) ? x[c] : T(0));
+    return j + 1 < L.ny ? x[c + L.nx] : ((L.neumann & 8u) ? x[c] : T(0));
+  }
+  const int plane = L.nx * L.ny;
+  if (dir < 0) return k > 0 ? x[c - plane] : ((L.neumann & 16u) ? x[c] : T(0));
+  return k + 1 < L.nz ? x[c + plane] : ((L.neumann & 32u) ? x[c] : T(0));
+}
+
+// Row s of the line system through cell (fa, fb) along `axis`: the same
+// a, b, c, d the Thomas solve forms (src/solver_mg.cpp:3440-3478).
+template <class T>
+__device__ __forceinline__ void line_row(const Level<T>& L,
+                                         const T* __restrict__ x,
+                                         const T* __restrict__ rhs, int axis,
+                                         int fa, int fb, int s, int& c, T& a,
+                                         T& bb, T& cc, T& d) {
+  const int extent = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+  const int plane = L.nx * L.ny;
+  const int i = axis == 0 ? s : fa;
+  const int j = axis == 0 ? fa : (axis == 1 ? s : fb);
+  const int k = axis == 2 ? s : fb;
+  c = i + L.nx * (j + L.ny * k);
+  const int fxi = face_x_index(L, c, j, k);
+  const int fyi = face_y_index(L, c, k);
+  T lowf, highf;
+  if (axis == 0) { lowf = L.fx[fxi]; highf = L.fx[fxi + 1]; }
+  else if (axis == 1) { lowf = L.fy[fyi]; highf = L.fy[fyi + L.nx]; }
+  else { lowf = L.fz[c]; highf = L.fz[c + plane]; }
+  a = s == 0 ? T(0) : -lowf;
+  bb = L.diag[c];
+  cc = s + 1 == extent ? T(0) : -highf;
+  d = rhs[c];
+  if (axis != 0) {
+    d += L.fx[fxi] * line_neighbour(L, x, i, j, k, c, 0, -1);
+    d += L.fx[fxi + 1] * line_neighbour(L, x, i, j, k, c, 0, 1);
+  }
+  if (axis != 1) {
+    d += L.fy[fyi] * line_neighbour(L, x, i, j, k, c, 1, -1);
+    d += L.fy[fyi + L.nx] * line_neighbour(L, x, i, j, k, c, 1, 1);
+  }
+  if (axis != 2) {
+    d += L.fz[c] * line_neighbour(L, x, i, j, k, c, 2, -1);
+    d += L.fz[c + plane] * line_neighbour(L, x, i, j, k, c, 2, 1);
+  }
+  if (s == 0) d += lowf * line_neighbour(L, x, i, j, k, c, axis, -1);
+  if (s + 1 == extent) d += highf * line_neighbour(L, x, i, j, k, c, axis, 1);
+}
+
+// Block-wide sum of up to three doubles; result valid in thread 0.
+template <int N>
+__device__ __forceinline__ void block_sum(double (&v)[N]) {
+  __shared__ double scratch[32][N];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int n = 0; n < N; ++n) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[n] += __shfl_down_sync(0xffffffffu, v[n], o);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) scratch[warp][n] = v[n];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) {
+      v[n] = lane < nwarps ? scratch[lane][n] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[n] += __shfl_down_sync(0xffffffffu, v[n], o);
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace hfps

@@ -1,0 +1,1139 @@
+// sm_100a kernels of the pressure solve: level stencils, smoothers, grid
+// transfers, Krylov vector kernels with fused deterministic reductions, and
+// the hierarchy setup.  Each kernel names the reference loop it replaces
+// (paths relative to versions/v0.4 of the reference).
+//
+// All of it is HBM-bound integer-indexed stencil work (about 0.27 flop per
+// byte): kernels read each operand once with coalesced x-fastest accesses,
+// neighbours come from L1/L2, and reductions use warp shuffles plus one
+// block pass, finished by the last block to arrive (fixed order, so every
+// sum is reproducible run to run).
+#include "kernels.hpp"
+
+#include <algorithm>
+#include <cmath>
+
+namespace hfps {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxReductionBlocks = 148 * 8;
+
+int grid_for(long long items) {
+  long long blocks = (items + kThreads - 1) / kThreads;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148LL * 32) blocks = 148LL * 32;
+  return static_cast<int>(blocks);
+}
+
+// Last block to finish reduces the per-block partials in block order and
+// applies the scalar update `op`.  Returns true in every thread of the last
+// block.
+template <int N>
+__device__ bool finish_reduction(double (&v)[N], const Reduce& red) {
+  block_sum<N>(v);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) red.partials[blockIdx.x * N + n] = v[n];
+    __threadfence();
+    const unsigned done = atomicAdd(&red.scalars->counters[red.op], 1u);
+    last = done == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  // Fixed-order final pass: thread t sums partials t, t+blockDim, ...
+  double acc[N];
+#pragma unroll
+  for (int n = 0; n < N; ++n) acc[n] = 0.0;
+  for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x) {
+#pragma unroll
+    for (int n = 0; n < N; ++n)
+      acc[n] += reinterpret_cast<volatile double*>(red.partials)[b * N + n];
+  }
+  block_sum<N>(acc);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int n = 0; n < N; ++n) v[n] = acc[n];
+    red.scalars->counters[red.op] = 0u;
+  }
+  return true;
+}
+
+__device__ void apply_scalar_op(Scalars* sc, int op, double sum) {
+  switch (op) {
+    case kOpPap: {
+      sc->pap = sum;
+      const double alpha = sc->rho / sum;
+      sc->alpha = alpha;
+      if (!(sum > 0.0) || !isfinite(sum)) sc->flags |= 2;
+      if (!isfinite(alpha)) sc->flags |= 1;
+      break;
+    }
+    case kOpRecursive:
+      sc->rr = sum;
+      if (!isfinite(sum)) sc->flags |= 1;
+      break;
+    case kOpRhoNext: {
+      sc->rho_next = sum;
+      if (!(sum > 0.0) || !isfinite(sum)) sc->flags |= 2;
+      sc->beta = sum / sc->rho;
+      sc->rho = sum;
+      break;
+    }
+    case kOpRhoRestart:
+      sc->rho_next = sum;
+      if (!(sum > 0.0) || !isfinite(sum)) sc->flags |= 2;
+      sc->rho = sum;
+      sc->beta = 0.0;
+      break;
+    default:
+      sc->misc[0] = sum;
+      if (!isfinite(sum)) sc->flags |= 1;
+      break;
+  }
+}
+
+__device__ __forceinline__ void cell_coords(int c, int nx, int ny, int& i,
+                                            int& j, int& k) {
+  const int row = c / nx;
+  i = c - row * nx;
+  k = row / ny;
+  j = row - k * ny;
+}
+
+// ---------------------------------------------------------------------------
+// Level operators: apply_level_matrix / apply_level_defect
+// (src/solver_mg.cpp:2569-2767).
+template <class T>
+__global__ void k_level_apply(Level<T> L, const T* __restrict__ x,
+                              T* __restrict__ y) {
+  const int n = L.nx * L.ny * L.nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    y[c] = row_value(L, x, i, j, k, c);
+  }
+}
+
+template <class T>
+__global__ void k_level_defect(Level<T> L, const T* __restrict__ x,
+                               const T* __restrict__ b, T* __restrict__ r) {
+  const int n = L.nx * L.ny * L.nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    r[c] = b[c] - row_value(L, x, i, j, k, c);
+  }
+}
+
+// Damped red-black Gauss-Seidel colour pass, omega = 0.72
+// (fused_point_color_update, src/solver_mg.cpp:3149-3223).  Cells of one
+// colour only read the other colour (and themselves), so the pass is
+// order-independent and matches the reference's sequential loop exactly.
+template <class T>
+__global__ void k_rb_color(Level<T> L, T* __restrict__ x,
+                           const T* __restrict__ b, int color) {
+  const int hx = (L.nx + 1) >> 1;
+  const int n = hx * L.ny * L.nz;
+  const T omega = T(0.72);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += gridDim.x * blockDim.x) {
+    const int row = t / hx;
+    const int ih = t - row * hx;
+    const int k = row / L.ny;
+    const int j = row - k * L.ny;
+    const int i = 2 * ih + ((j + k + color) & 1);
+    if (i >= L.nx) continue;
+    const int c = i + L.nx * row;
+    const T value = row_value(L, x, i, j, k, c);
+    x[c] += omega * (b[c] - value) / L.diag[c];
+  }
+}
+
+// One Chebyshev-Jacobi stage (chebyshev_stream_bulk_kernel,
+// src/solver_mg.cpp:2464-2490): d = f_prev d + f_res (b - A x)/D, x' = x + d.
+template <class T>
+__global__ void k_chebyshev_stage(Level<T> L, const T* __restrict__ x,
+                                  const T* __restrict__ b,
+                                  T* __restrict__ direction,
+                                  T* __restrict__ next, T previous_factor,
+                                  T residual_factor, int first) {
+  const int n = L.nx * L.ny * L.nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    const T value = row_value(L, x, i, j, k, c);
+    const T defect = b[c] - value;
+    const T scaled = residual_factor * defect / L.diag[c];
+    const T d = first ? scaled : previous_factor * direction[c] + scaled;
+    direction[c] = d;
+    next[c] = x[c] + d;
+  }
+}
+
+// Thomas solve of one line (solve_one, src/solver_mg.cpp:3388-3493).
+template <class T>
+__device__ void line_thomas(const Level<T>& L, T* __restrict__ x,
+                            const T* __restrict__ b, T* __restrict__ work,
+                            T* __restrict__ dprime, int axis, int fa,
+                            int fb) {
+  const int extent = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
+  const int plane = L.nx * L.ny;
+  const int stride = axis == 0 ? 1 : (axis == 1 ? L.nx : plane);
+  int i0, j0, k0;
+  if (axis == 0) { i0 = 0; j0 = fa; k0 = fb; }
+  else if (axis == 1) { i0 = fa; j0 = 0; k0 = fb; }
+  else { i0 = fa; j0 = fb; k0 = 0; }
+  const int c0 = i0 + L.nx * (j0 + L.ny * k0);
+  T prev_work = T(0), prev_d = T(0);
+  for (int s = 0; s < extent; ++s) {
+    const int i = axis == 0 ? s : i0;
+    const int j = axis == 1 ? s : j0;
+    const int k = axis == 2 ? s : k0;
+    const int c = c0 + s * stride;
+    const int fxi = face_x_index(L, c, j, k);
+    const int fyi = face_y_index(L, c, k);
+    T lowf, highf;
+    if (axis == 0) { lowf = L.fx[fxi]; highf = L.fx[fxi + 1]; }
+    else if (axis == 1) { lowf = L.fy[fyi]; highf = L.fy[fyi + L.nx]; }
+    else { lowf = L.fz[c]; highf = L.fz[c + plane]; }
+    const T a = s == 0 ? T(0) : -lowf;
+    const T bb = L.diag[c];
+    const T cc = s + 1 == extent ? T(0) : -highf;
+    T d = b[c];
+    if (axis != 0) {
+      d += L.fx[fxi] * line_neighbour(L, x, i, j, k, c, 0, -1);
+      d += L.fx[fxi + 1] * line_neighbour(L, x, i, j, k, c, 0, 1);
+    }
+    if (axis != 1) {
+      d += L.fy[fyi] * line_neighbour(L, x, i, j, k, c, 1, -1);
+      d += L.fy[fyi + L.nx] * line_neighbour(L, x, i, j, k, c, 1, 1);
+    }
+    if (axis != 2) {
+      d += L.fz[c] * line_neighbour(L, x, i, j, k, c, 2, -1);
+      d += L.fz[c + plane] * line_neighbour(L, x, i, j, k, c, 2, 1);
+    }
+    if (s == 0) d += lowf * line_neighbour(L, x, i, j, k, c, axis, -1);
+    if (s + 1 == extent) d += highf * line_neighbour(L, x, i, j, k, c, axis, 1);
+    T wv, dv;
+    if (s > 0) {
+      const T denominator = bb - a * prev_work;
+      wv = cc / denominator;
+      dv = (d - a * prev_d) / denominator;
+    } else {
+      wv = cc / bb;
+      dv = d / bb;
+    }
+    work[c] = wv;
+    dprime[c] = dv;
+    prev_work = wv;
+    prev_d = dv;
+  }
+  T next_x = T(0);
+  for (int s = extent; s-- > 0;) {
+    const int c = c0 + s * stride;
+    const T v = s + 1 == extent ? dprime[c] : dprime[c] - work[c] * next_x;
+    x[c] = v;
+    next_x = v;
+  }
+}
+
+// Fused retained defect + restriction (apply_level_defect followed by
+// restrict_residual, src/solver_mg.cpp:3633-3721): every coarse cell sums
+// the defects of its children in dz, dy, dx order; coarse x is zeroed.
+template <class T>
+__global__ void k_defect_restrict(Level<T> F, const T* __restrict__ x,
+                                  const T* __restrict__ b, Level<T> C,
+                                  T* __restrict__ cb, T* __restrict__ cx,
+                                  int mask) {
+  const int n = C.nx * C.ny * C.nz;
+  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
+  for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
+       cc += gridDim.x * blockDim.x) {
+    int ci, cj, ck;
+    cell_coords(cc, C.nx, C.ny, ci, cj, ck);
+    const int xb = mx ? 2 * ci : ci, yb = my ? 2 * cj : cj, zb = mz ? 2 * ck : ck;
+    T sum = T(0);
+    for (int dz = 0; dz <= mz; ++dz)
+      for (int dy = 0; dy <= my; ++dy)
+        for (int dx = 0; dx <= mx; ++dx) {
+          const int fi = xb + dx, fj = yb + dy, fk = zb + dz;
+          if (fi >= F.nx || fj >= F.ny || fk >= F.nz) continue;
+          const int fc = fi + F.nx * (fj + F.ny * fk);
+          sum += b[fc] - row_value(F, x, fi, fj, fk, fc);
+        }
+    cb[cc] = sum;
+    cx[cc] = T(0);
+  }
+}
+
+template <class T>
+__global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
+                           T* __restrict__ cb, T* __restrict__ cx, int mask) {
+  const int n = C.nx * C.ny * C.nz;
+  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
+  for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
+       cc += gridDim.x * blockDim.x) {
+    int ci, cj, ck;
+    cell_coords(cc, C.nx, C.ny, ci, cj, ck);
+    const int xb = mx ? 2 * ci : ci, yb = my ? 2 * cj : cj, zb = mz ? 2 * ck : ck;
+    T sum = T(0);
+    for (int dz = 0; dz <= mz; ++dz)
+      for (int dy = 0; dy <= my; ++dy)
+        for (int dx = 0; dx <= mx; ++dx) {
+          const int fi = xb + dx, fj = yb + dy, fk = zb + dz;
+          if (fi >= F.nx || fj >= F.ny || fk >= F.nz) continue;
+          sum += r[fi + F.nx * (fj + F.ny * fk)];
+        }
+    cb[cc] = sum;
+    cx[cc] = T(0);
+  }
+}
+
+__device__ __forceinline__ void interp_axis(int fine, int coarsened,
+                                            int extent, int& left, int& right,
+                                            double& weight) {
+  if (!coarsened) {
+    left = right = fine;
+    weight = 0.0;
+    return;
+  }
+  const int parent = fine >> 1;
+  if ((fine & 1) == 0) {
+    left = parent - 1;
+    right = parent;
+    weight = 0.75;
+  } else {
+    left = parent;
+    right = parent + 1;
+    weight = 0.25;
+  }
+  if (left < 0) {
+    left = right = 0;
+    weight = 0.0;
+  } else if (right >= extent) {
+    left = right = extent - 1;
+    weight = 0.0;
+  }
+}
+
+// Trilinear prolongation and add, zero on solid cells (prolongate_add,
+// src/solver_mg.cpp:3893-3994).  Weights are formed in double exactly as
+// the reference does and rounded once to T for the FP32 hierarchy.
+template <class T>
+__global__ void k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C,
+                             const T* __restrict__ cx, int mask) {
+  const int n = F.nx * F.ny * F.nz;
+  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    if (F.fluid[c] == 0) {
+      x[c] = T(0);
+      continue;
+    }
+    int i, j, k;
+    cell_coords(c, F.nx, F.ny, i, j, k);
+    int xl, xr, yl, yr, zl, zr;
+    double xw, yw, zw;
+    interp_axis(i, mx, C.nx, xl, xr, xw);
+    interp_axis(j, my, C.ny, yl, yr, yw);
+    interp_axis(k, mz, C.nz, zl, zr, zw);
+    T value = T(0);
+    for (int az = 0; az < (zl == zr ? 1 : 2); ++az) {
+      const int gz = az == 0 ? zl : zr;
+      const double wz = az == 0 ? 1.0 - zw : zw;
+      for (int ay = 0; ay < (yl == yr ? 1 : 2); ++ay) {
+        const int gy = ay == 0 ? yl : yr;
+        const double wy = ay == 0 ? 1.0 - yw : yw;
+        for (int ax = 0; ax < (xl == xr ? 1 : 2); ++ax) {
+          const int gx = ax == 0 ? xl : xr;
+          const double wx = ax == 0 ? 1.0 - xw : xw;
+          const T w = static_cast<T>(wx * wy * wz);
+          value += w * cx[gx + C.nx * (gy + C.ny * gz)];
+        }
+      }
+    }
+    x[c] += value;
+  }
+}
+
+// Coarsest level: `sweeps` smoother sweeps in one CTA (mg_cycle coarse
+// branch, src/solver_mg.cpp:4210-4227).  The state is widened to TC (FP64
+// in the mixed-precision hierarchy) for the duration of the solve.
+template <class T, class TC>
+__global__ void k_coarse_solve(Level<TC> L, T* __restrict__ x,
+                               const T* __restrict__ b, TC* __restrict__ xs,
+                               TC* __restrict__ bs, TC* __restrict__ work,
+                               TC* __restrict__ dprime, int sweeps,
+                               int line_axis) {
+  const int n = L.nx * L.ny * L.nz;
+  TC* xw = xs;
+  const TC* bw = bs;
+  if (xs != nullptr) {
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      xs[c] = static_cast<TC>(x[c]);
+      bs[c] = static_cast<TC>(b[c]);
+    }
+    __syncthreads();
+  } else {
+    xw = reinterpret_cast<TC*>(x);
+    bw = reinterpret_cast<const TC*>(b);
+  }
+  if (line_axis < 0) {
+    const TC omega = TC(0.72);
+    const int hx = (L.nx + 1) >> 1;
+    const int half = hx * L.ny * L.nz;
+    for (int s = 0; s < sweeps; ++s) {
+      for (int color = 0; color < 2; ++color) {
+        for (int t = threadIdx.x; t < half; t += blockDim.x) {
+          const int row = t / hx;
+          const int ih = t - row * hx;
+          const int k = row / L.ny;
+          const int j = row - k * L.ny;
+          const int i = 2 * ih + ((j + k + color) & 1);
+          if (i >= L.nx) continue;
+          const int c = i + L.nx * row;
+          const TC value = row_value(L, xw, i, j, k, c);
+          xw[c] += omega * (bw[c] - value) / L.diag[c];
+        }
+        __syncthreads();
+      }
+    }
+  } else {
+    const int a_extent = line_axis == 0 ? L.ny : L.nx;
+    const int b_extent = line_axis == 2 ? L.ny : L.nz;
+    const int ha = (a_extent + 1) >> 1;
+    const int lines = ha * b_extent;
+    for (int s = 0; s < sweeps; ++s) {
+      for (int color = 0; color < 2; ++color) {
+        for (int t = threadIdx.x; t < lines; t += blockDim.x) {
+          const int fb = t / ha;
+          const int fa = 2 * (t - fb * ha) + ((fb + color) & 1);
+          if (fa >= a_extent) continue;
+          line_thomas(L, xw, bw, work, dprime, line_axis, fa, fb);
+        }
+        __syncthreads();
+      }
+    }
+  }
+  if (xs != nullptr) {
+    for (int c = threadIdx.x; c < n; c += blockDim.x) x[c] = static_cast<T>(xs[c]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MG entry/exit (apply_impl, src/solver_mg.cpp:4866-4878, 5078-5117).
+template <class T>
+__global__ void k_mg_enter(int n, const double* __restrict__ r,
+                           const uint8_t* __restrict__ active,
+                           T* __restrict__ b, T* __restrict__ x) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const bool on = active == nullptr || active[c] != 0;
+    b[c] = on ? static_cast<T>(r[c]) : T(0);
+    x[c] = T(0);
+  }
+}
+
+template <class T>
+__global__ void k_mg_exit(int n, const T* __restrict__ x,
+                          const uint8_t* __restrict__ active,
+                          const double* __restrict__ scale_ptr,
+                          double* __restrict__ z) {
+  const double scale = scale_ptr == nullptr ? 1.0 : *scale_ptr;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const bool on = active == nullptr || active[c] != 0;
+    z[c] = on ? static_cast<double>(x[c]) * scale : 0.0;
+  }
+}
+
+template <class T>
+__global__ void k_diagonal_solve(int n, const T* __restrict__ b,
+                                 const T* __restrict__ diag,
+                                 T* __restrict__ x) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x)
+    x[c] = b[c] / diag[c];
+}
+
+template <class T>
+__global__ void k_mg_projection(int n, const double* __restrict__ r_in,
+                                const uint8_t* __restrict__ active,
+                                const T* __restrict__ recursive, Reduce red) {
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const bool on = active == nullptr || active[c] != 0;
+    const double r = on ? r_in[c] : 0.0;
+    const double az = r - static_cast<double>(recursive[c]);
+    v[0] += r * r;
+    v[1] += r * az;
+    v[2] += az * az;
+  }
+  if (finish_reduction<3>(v, red) && threadIdx.x == 0) {
+    Scalars* sc = red.scalars;
+    sc->proj[0] = v[0];
+    sc->proj[1] = v[1];
+    sc->proj[2] = v[2];
+    const double tiny = 2.220446049250313e-16 * v[0];
+    sc->mg_alpha = v[2] > tiny ? v[1] / v[2] : 0.0;
+    if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2]) ||
+        !isfinite(sc->mg_alpha))
+      sc->flags |= 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Krylov kernels (FP64).  solve_pcg's operator apply + p.Ap
+// (src/solver_krylov.cpp:1426-1447), x/r update + recursive norm
+// (:1448-1463), r.z (:1536-1540) and p = z + beta p (:1546).
+__global__ void k_spmv_dot(Level<double> L, const double* __restrict__ x,
+                           double* __restrict__ y, Reduce red) {
+  const int n = L.nx * L.ny * L.nz;
+  double v[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    const double a = row_value(L, x, i, j, k, c);
+    y[c] = a;
+    v[0] += x[c] * a;
+  }
+  if (finish_reduction<1>(v, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, v[0]);
+}
+
+__global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
+                                const double* __restrict__ b,
+                                double* __restrict__ r, Reduce red) {
+  const int n = L.nx * L.ny * L.nz;
+  double v[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    const double value = b[c] - row_value(L, x, i, j, k, c);
+    r[c] = value;
+    v[0] += value * value;
+  }
+  if (finish_reduction<1>(v, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, v[0]);
+}
+
+__global__ void k_pcg_update(int n, double* __restrict__ x,
+                             const double* __restrict__ p,
+                             double* __restrict__ r,
+                             const double* __restrict__ ap, Reduce red) {
+  const double alpha = red.scalars->alpha;
+  double v[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    x[c] = x[c] + alpha * p[c];
+    const double rv = r[c] + -alpha * ap[c];
+    r[c] = rv;
+    v[0] += rv * rv;
+  }
+  if (finish_reduction<1>(v, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, v[0]);
+}
+
+__global__ void k_dot(int n, const double* __restrict__ a,
+                      const double* __restrict__ b, Reduce red) {
+  double v[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x)
+    v[0] += a[c] * b[c];
+  if (finish_reduction<1>(v, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, v[0]);
+}
+
+__global__ void k_norm2(int n, const double* __restrict__ a, Reduce red) {
+  double v[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x)
+    v[0] += a[c] * a[c];
+  if (finish_reduction<1>(v, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, v[0]);
+}
+
+__global__ void k_p_update(int n, double* __restrict__ p,
+                           const double* __restrict__ z,
+                           const Scalars* __restrict__ sc) {
+  const double beta = sc->beta;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x)
+    p[c] = 1.0 * z[c] + beta * p[c];
+}
+
+__global__ void k_copy(int n, const double* __restrict__ src,
+                       double* __restrict__ dst) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x)
+    dst[c] = src[c];
+}
+
+// ---------------------------------------------------------------------------
+// Setup: copy_finest_coefficients (src/solver_mg.cpp:1469-1570).  A face is
+// active iff every adjacent cell is fluid; solid rows become identities; a
+// fluid diagonal loses exactly the removed face coefficients.
+__device__ __forceinline__ bool cell_on(const uint8_t* a, int c) {
+  return a == nullptr || a[c] != 0;
+}
+
+__global__ void k_mask_faces(int nx, int ny, int nz, const double* fx_in,
+                             const double* fy_in, const double* fz_in,
+                             const uint8_t* active, double* fx, double* fy,
+                             double* fz) {
+  const int nfx = (nx + 1) * ny * nz;
+  const int nfy = nx * (ny + 1) * nz;
+  const int nfz = nx * ny * (nz + 1);
+  const int total = nfx + nfy + nfz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += gridDim.x * blockDim.x) {
+    if (t < nfx) {
+      const int row = t / (nx + 1);
+      const int i = t - row * (nx + 1);
+      const int base = nx * row;
+      bool on = true;
+      if (i > 0) on = on && cell_on(active, base + i - 1);
+      if (i < nx) on = on && cell_on(active, base + i);
+      fx[t] = fx_in[t] * (on ? 1.0 : 0.0);
+    } else if (t < nfx + nfy) {
+      const int f = t - nfx;
+      const int i = f % nx;
+      const int r = f / nx;  // j + (ny+1) k
+      const int k = r / (ny + 1);
+      const int j = r - k * (ny + 1);
+      bool on = true;
+      if (j > 0) on = on && cell_on(active, i + nx * (j - 1 + ny * k));
+      if (j < ny) on = on && cell_on(active, i + nx * (j + ny * k));
+      fy[f] = fy_in[f] * (on ? 1.0 : 0.0);
+    } else {
+      const int f = t - nfx - nfy;
+      const int plane = nx * ny;
+      const int k = f / plane;
+      const int rem = f - k * plane;
+      bool on = true;
+      if (k > 0) on = on && cell_on(active, rem + plane * (k - 1));
+      if (k < nz) on = on && cell_on(active, rem + plane * k);
+      fz[f] = fz_in[f] * (on ? 1.0 : 0.0);
+    }
+  }
+}
+
+__global__ void k_mask_cells(int nx, int ny, int nz, const double* x_faces,
+                             const double* y_faces, const double* z_faces,
+                             const double* diag_in, const double* fx_in,
+                             const double* fy_in, const double* fz_in,
+                             const uint8_t* active, double* diag,
+                             const double* fx, const double* fy,
+                             const double* fz, double* volume,
+                             uint8_t* fluid) {
+  const int n = nx * ny * nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, nx, ny, i, j, k);
+    const bool on = cell_on(active, c);
+    double vol = (x_faces[i + 1] - x_faces[i]) * (y_faces[j + 1] - y_faces[j]) *
+                 (z_faces[k + 1] - z_faces[k]);
+    if (!on) vol = 0.0;
+    volume[c] = vol;
+    fluid[c] = vol > 0.0 ? 1 : 0;
+    double d = diag_in[c];
+    if (active != nullptr) {
+      if (!on) {
+        d = 1.0;
+      } else {
+        const int fxi = c + j + ny * k;
+        const int fyi = c + nx * k;
+        const int plane = nx * ny;
+        const double original = fx_in[fxi] + fx_in[fxi + 1] + fy_in[fyi] +
+                                fy_in[fyi + nx] + fz_in[c] + fz_in[c + plane];
+        const double act = fx[fxi] + fx[fxi + 1] + fy[fyi] + fy[fyi + nx] +
+                           fz[c] + fz[c + plane];
+        d = d - original + act;
+      }
+    }
+    diag[c] = d;
+  }
+}
+
+// Per fine cell: max(0, diag - sum of faces) for fluid cells, the reaction
+// aggregated into the coarse diagonal (src/solver_mg.cpp:1880-1894).
+__global__ void k_reaction(Level<double> L, const double* volume,
+                           double* reaction) {
+  const int n = L.nx * L.ny * L.nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    if (volume[c] == 0.0) {
+      reaction[c] = 0.0;
+      continue;
+    }
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    const int fxi = face_x_index(L, c, j, k);
+    const int fyi = face_y_index(L, c, k);
+    const int plane = L.nx * L.ny;
+    const double faces = L.fx[fxi] + L.fx[fxi + 1] + L.fy[fyi] +
+                         L.fy[fyi + L.nx] + L.fz[c] + L.fz[c + plane];
+    const double v = L.diag[c] - faces;
+    reaction[c] = v > 0.0 ? v : 0.0;
+  }
+}
+
+// One axis of aggregate_tensor_channel (src/solver_mg.cpp:1790-1838):
+// normal faces copy fine face min(2c, extent); cells and tangential faces
+// sum their (at most) two children.
+__global__ void k_aggregate_axis(const double* src, int ex, int ey, int ez,
+                                 double* dst, int dx, int dy, int dz, int axis,
+                                 int face_axis, int global_extent) {
+  const int n = dx * dy * dz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += gridDim.x * blockDim.x) {
+    int o[3];
+    cell_coords(t, dx, dy, o[0], o[1], o[2]);
+    double value = 0.0;
+    if (face_axis == axis) {
+      int fg = 2 * o[axis];
+      if (fg > global_extent) fg = global_extent;
+      int s[3] = {o[0], o[1], o[2]};
+      s[axis] = fg;
+      value = src[s[0] + ex * (s[1] + ey * s[2])];
+    } else {
+      for (int child = 0; child < 2; ++child) {
+        const int fg = 2 * o[axis] + child;
+        if (fg >= global_extent) continue;
+        int s[3] = {o[0], o[1], o[2]};
+        s[axis] = fg;
+        value += src[s[0] + ex * (s[1] + ey * s[2])];
+      }
+    }
+    dst[t] = value;
+  }
+  (void)ez;
+}
+
+__global__ void k_coarse_diagonal(int nx, int ny, int nz, double* diag,
+                                  const double* fx, const double* fy,
+                                  const double* fz, const double* volume,
+                                  uint8_t* fluid) {
+  const int n = nx * ny * nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, nx, ny, i, j, k);
+    const int fxi = c + j + ny * k;
+    const int fyi = c + nx * k;
+    const int plane = nx * ny;
+    double d = diag[c];
+    d += fx[fxi] + fx[fxi + 1] + fy[fyi] + fy[fyi + nx] + fz[c] + fz[c + plane];
+    if (volume[c] == 0.0) d = 1.0;
+    diag[c] = d;
+    fluid[c] = volume[c] > 0.0 ? 1 : 0;
+  }
+}
+
+// face_pressure_coefficient (src/solver_piso.cpp:1060-1136) from cell beta.
+__global__ void k_beta_faces(int nx, int ny, int nz, const double* xf,
+                             const double* yf, const double* zf,
+                             unsigned neumann, const double* beta, double* fx,
+                             double* fy, double* fz) {
+  const int nfx = (nx + 1) * ny * nz;
+  const int nfy = nx * (ny + 1) * nz;
+  const int nfz = nx * ny * (nz + 1);
+  const int total = nfx + nfy + nfz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += gridDim.x * blockDim.x) {
+    int axis, f, i, j, k, n_axis;
+    const double* faces;
+    if (t < nfx) {
+      axis = 0; f = t; n_axis = nx; faces = xf;
+      const int row = f / (nx + 1);
+      i = f - row * (nx + 1);
+      k = row / ny;
+      j = row - k * ny;
+    } else if (t < nfx + nfy) {
+      axis = 1; f = t - nfx; n_axis = ny; faces = yf;
+      i = f % nx;
+      const int r = f / nx;
+      k = r / (ny + 1);
+      j = r - k * (ny + 1);
+    } else {
+      axis = 2; f = t - nfx - nfy; n_axis = nz; faces = zf;
+      const int plane = nx * ny;
+      k = f / plane;
+      const int rem = f - k * plane;
+      j = rem / nx;
+      i = rem - j * nx;
+    }
+    const int normal = axis == 0 ? i : (axis == 1 ? j : k);
+    double area;
+    if (axis == 0) area = (yf[j + 1] - yf[j]) * (zf[k + 1] - zf[k]);
+    else if (axis == 1) area = (xf[i + 1] - xf[i]) * (zf[k + 1] - zf[k]);
+    else area = (xf[i + 1] - xf[i]) * (yf[j + 1] - yf[j]);
+    const auto cell = [&](int nn) {
+      int a = i, b = j, cc = k;
+      if (axis == 0) a = nn; else if (axis == 1) b = nn; else cc = nn;
+      return a + nx * (b + ny * cc);
+    };
+    double value;
+    if (normal == 0 || normal == n_axis) {
+      const bool high = normal == n_axis;
+      const bool is_neumann = (neumann >> (2 * axis + (high ? 1 : 0))) & 1u;
+      if (is_neumann) {
+        value = 0.0;
+      } else {
+        const int owner = cell(high ? n_axis - 1 : 0);
+        const double centre = 0.5 * (faces[high ? n_axis - 1 : 0] + faces[high ? n_axis : 1]);
+        const double d = high ? faces[n_axis] - centre : centre - faces[0];
+        const double inv = 1.0 / beta[owner];
+        value = 2.0 * area / (d * inv + d * inv);
+      }
+    } else {
+      const double cl = 0.5 * (faces[normal - 1] + faces[normal]);
+      const double cr = 0.5 * (faces[normal] + faces[normal + 1]);
+      const double dl = faces[normal] - cl;
+      const double dr = cr - faces[normal];
+      value = area / (dl / beta[cell(normal - 1)] + dr / beta[cell(normal)]);
+    }
+    if (axis == 0) fx[f] = value; else if (axis == 1) fy[f] = value; else fz[f] = value;
+  }
+}
+
+__global__ void k_beta_diagonal(int nx, int ny, int nz, const double* fx,
+                                const double* fy, const double* fz,
+                                const double* storage, double* diag) {
+  const int n = nx * ny * nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, nx, ny, i, j, k);
+    const int fxi = c + j + ny * k;
+    const int fyi = c + nx * k;
+    const int plane = nx * ny;
+    double d = storage == nullptr ? 0.0 : storage[c];
+    d += fx[fxi] + fx[fxi + 1] + fy[fyi] + fy[fyi + nx] + fz[c] + fz[c + plane];
+    diag[c] = d;
+  }
+}
+
+__global__ void k_shortcut_ratio(Level<double> L, Reduce red) {
+  const int n = L.nx * L.ny * L.nz;
+  double v[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    const int fxi = face_x_index(L, c, j, k);
+    const int fyi = face_y_index(L, c, k);
+    const int plane = L.nx * L.ny;
+    const double sum = L.fx[fxi] + L.fx[fxi + 1] + L.fy[fyi] +
+                       L.fy[fyi + L.nx] + L.fz[c] + L.fz[c + plane];
+    v[0] = fmax(v[0], sum / L.diag[c]);
+  }
+  // max reduction: reuse the partial buffer with a fixed-order max.
+  __shared__ double scratch[kThreads];
+  scratch[threadIdx.x] = v[0];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) scratch[threadIdx.x] = fmax(scratch[threadIdx.x], scratch[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) red.partials[blockIdx.x] = scratch[0];
+}
+
+template <class TO, class TI>
+__global__ void k_convert(size_t n, const TI* __restrict__ src,
+                          TO* __restrict__ dst) {
+  for (size_t c = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+       c < n; c += static_cast<size_t>(gridDim.x) * blockDim.x)
+    dst[c] = static_cast<TO>(src[c]);
+}
+
+// Adjoint face gradients: dL/dc_f = -(l_i - l_j)(p_i - p_j) on active
+// interior faces, -l_i p_i on Dirichlet boundary faces, 0 elsewhere.
+__global__ void k_face_gradients(Level<double> L, const double* lambda,
+                                 const double* p, double* gx, double* gy,
+                                 double* gz) {
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const int nfx = (nx + 1) * ny * nz;
+  const int nfy = nx * (ny + 1) * nz;
+  const int nfz = nx * ny * (nz + 1);
+  const int total = nfx + nfy + nfz;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += gridDim.x * blockDim.x) {
+    int axis, f, lo = -1, hi = -1, normal, n_axis;
+    if (t < nfx) {
+      axis = 0; f = t; n_axis = nx;
+      const int row = f / (nx + 1);
+      const int i = f - row * (nx + 1);
+      normal = i;
+      if (i > 0) lo = nx * row + i - 1;
+      if (i < nx) hi = nx * row + i;
+    } else if (t < nfx + nfy) {
+      axis = 1; f = t - nfx; n_axis = ny;
+      const int i = f % nx;
+      const int r = f / nx;
+      const int k = r / (ny + 1);
+      const int j = r - k * (ny + 1);
+      normal = j;
+      if (j > 0) lo = i + nx * (j - 1 + ny * k);
+      if (j < ny) hi = i + nx * (j + ny * k);
+    } else {
+      axis = 2; f = t - nfx - nfy; n_axis = nz;
+      const int plane = nx * ny;
+      const int k = f / plane;
+      const int rem = f - k * plane;
+      normal = k;
+      if (k > 0) lo = rem + plane * (k - 1);
+      if (k < nz) hi = rem + plane * k;
+    }
+    double g = 0.0;
+    if (lo >= 0 && hi >= 0) {
+      if (L.fluid[lo] && L.fluid[hi]) g = -(lambda[lo] - lambda[hi]) * (p[lo] - p[hi]);
+    } else {
+      const int owner = lo >= 0 ? lo : hi;
+      const bool high = normal == n_axis;
+      const bool is_neumann = (L.neumann >> (2 * axis + (high ? 1 : 0))) & 1u;
+      if (!is_neumann && L.fluid[owner]) g = -lambda[owner] * p[owner];
+    }
+    if (axis == 0) gx[f] = g; else if (axis == 1) gy[f] = g; else gz[f] = g;
+  }
+}
+
+__global__ void k_adjoint_source(int n, const double* dl_dp,
+                                 const uint8_t* active, double* out) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x)
+    out[c] = cell_on(active, c) ? dl_dp[c] : 0.0;
+}
+
+}  // namespace
+
+int reduction_blocks(long long items) {
+  long long blocks = (items + kThreads - 1) / kThreads;
+  if (blocks < 1) blocks = 1;
+  if (blocks > kMaxReductionBlocks) blocks = kMaxReductionBlocks;
+  return static_cast<int>(blocks);
+}
+
+// ---- launchers ---------------------------------------------------------------
+#define HFPS_CELLS(L) (static_cast<long long>((L).nx) * (L).ny * (L).nz)
+
+template <class T>
+void launch_level_apply(cudaStream_t s, const Level<T>& L, const T* x, T* y) {
+  k_level_apply<T><<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, y);
+}
+template <class T>
+void launch_level_defect(cudaStream_t s, const Level<T>& L, const T* x,
+                         const T* b, T* r) {
+  k_level_defect<T><<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, b, r);
+}
+template <class T>
+void launch_rb_color(cudaStream_t s, const Level<T>& L, T* x, const T* b,
+                     int color) {
+  const long long half = static_cast<long long>((L.nx + 1) / 2) * L.ny * L.nz;
+  k_rb_color<T><<<grid_for(half), kThreads, 0, s>>>(L, x, b, color);
+}
+template <class T>
+void launch_chebyshev_stage(cudaStream_t s, const Level<T>& L, const T* x,
+                            const T* b, T* direction, T* next,
+                            T previous_factor, T residual_factor, int first) {
+  k_chebyshev_stage<T><<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(
+      L, x, b, direction, next, previous_factor, residual_factor, first);
+}
+template <class T>
+void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
+                            const T* b, const Level<T>& C, T* cb, T* cx,
+                            int mask) {
+  k_defect_restrict<T><<<grid_for(HFPS_CELLS(C)), kThreads, 0, s>>>(F, x, b, C, cb,
+                                                                   cx, mask);
+}
+template <class T>
+void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
+                     const Level<T>& C, T* cb, T* cx, int mask) {
+  k_restrict<T><<<grid_for(HFPS_CELLS(C)), kThreads, 0, s>>>(F, r, C, cb, cx, mask);
+}
+template <class T>
+void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
+                       const Level<T>& C, const T* cx, int mask) {
+  k_prolongate<T><<<grid_for(HFPS_CELLS(F)), kThreads, 0, s>>>(F, x, C, cx, mask);
+}
+template <class T, class TC>
+void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
+                         TC* xs, TC* bs, TC* work, TC* dprime, int sweeps,
+                         int line_axis) {
+  k_coarse_solve<T, TC><<<1, 512, 0, s>>>(L, x, b, xs, bs, work, dprime, sweeps,
+                                          line_axis);
+}
+template <class T>
+void launch_mg_enter(cudaStream_t s, int n, const double* r,
+                     const uint8_t* active, T* b, T* x) {
+  k_mg_enter<T><<<grid_for(n), kThreads, 0, s>>>(n, r, active, b, x);
+}
+template <class T>
+void launch_mg_exit(cudaStream_t s, int n, const T* x, const uint8_t* active,
+                    const double* scale_ptr, double* z) {
+  k_mg_exit<T><<<grid_for(n), kThreads, 0, s>>>(n, x, active, scale_ptr, z);
+}
+template <class T>
+void launch_diagonal_solve(cudaStream_t s, int n, const T* b, const T* diag,
+                           T* x) {
+  k_diagonal_solve<T><<<grid_for(n), kThreads, 0, s>>>(n, b, diag, x);
+}
+template <class T>
+void launch_mg_projection(cudaStream_t s, int n, const double* r,
+                          const uint8_t* active, const T* recursive,
+                          Reduce red) {
+  k_mg_projection<T><<<reduction_blocks(n), kThreads, 0, s>>>(n, r, active,
+                                                              recursive, red);
+}
+
+void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
+                     double* y, Reduce red) {
+  k_spmv_dot<<<reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, y, red);
+}
+void launch_residual_norm(cudaStream_t s, const Level<double>& L,
+                          const double* x, const double* b, double* r,
+                          Reduce red) {
+  k_residual_norm<<<reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, b, r,
+                                                                       red);
+}
+void launch_pcg_update(cudaStream_t s, int n, double* x, const double* p,
+                       double* r, const double* ap, Reduce red) {
+  k_pcg_update<<<reduction_blocks(n), kThreads, 0, s>>>(n, x, p, r, ap, red);
+}
+void launch_dot(cudaStream_t s, int n, const double* a, const double* b,
+                Reduce red) {
+  k_dot<<<reduction_blocks(n), kThreads, 0, s>>>(n, a, b, red);
+}
+void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red) {
+  k_norm2<<<reduction_blocks(n), kThreads, 0, s>>>(n, v, red);
+}
+void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
+                     const Scalars* sc) {
+  k_p_update<<<grid_for(n), kThreads, 0, s>>>(n, p, z, sc);
+}
+void launch_copy(cudaStream_t s, int n, const double* src, double* dst) {
+  k_copy<<<grid_for(n), kThreads, 0, s>>>(n, src, dst);
+}
+
+void launch_mask_finest(cudaStream_t s, int nx, int ny, int nz,
+                        const double* x_faces, const double* y_faces,
+                        const double* z_faces, const double* diag_in,
+                        const double* fx_in, const double* fy_in,
+                        const double* fz_in, const uint8_t* active,
+                        double* diag, double* fx, double* fy, double* fz,
+                        double* volume, uint8_t* fluid) {
+  const long long faces = static_cast<long long>(nx + 1) * ny * nz +
+                          static_cast<long long>(nx) * (ny + 1) * nz +
+                          static_cast<long long>(nx) * ny * (nz + 1);
+  k_mask_faces<<<grid_for(faces), kThreads, 0, s>>>(nx, ny, nz, fx_in, fy_in, fz_in,
+                                                    active, fx, fy, fz);
+  k_mask_cells<<<grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s>>>(
+      nx, ny, nz, x_faces, y_faces, z_faces, diag_in, fx_in, fy_in, fz_in, active,
+      diag, fx, fy, fz, volume, fluid);
+}
+void launch_reaction(cudaStream_t s, const Level<double>& L,
+                     const double* volume, double* reaction) {
+  k_reaction<<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(L, volume, reaction);
+}
+void launch_aggregate_axis(cudaStream_t s, const double* src, int ex, int ey,
+                           int ez, double* dst, int dx, int dy, int dz,
+                           int axis, int face_axis, int global_extent) {
+  k_aggregate_axis<<<grid_for(static_cast<long long>(dx) * dy * dz), kThreads, 0,
+                     s>>>(src, ex, ey, ez, dst, dx, dy, dz, axis, face_axis,
+                          global_extent);
+}
+void launch_coarse_diagonal(cudaStream_t s, int nx, int ny, int nz,
+                            double* diag, const double* fx, const double* fy,
+                            const double* fz, const double* volume,
+                            uint8_t* fluid) {
+  k_coarse_diagonal<<<grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0,
+                      s>>>(nx, ny, nz, diag, fx, fy, fz, volume, fluid);
+}
+void launch_beta_coefficients(cudaStream_t s, int nx, int ny, int nz,
+                              const double* x_faces, const double* y_faces,
+                              const double* z_faces, unsigned neumann,
+                              const double* beta, const double* storage,
+                              double* diag, double* fx, double* fy,
+                              double* fz) {
+  const long long faces = static_cast<long long>(nx + 1) * ny * nz +
+                          static_cast<long long>(nx) * (ny + 1) * nz +
+                          static_cast<long long>(nx) * ny * (nz + 1);
+  k_beta_faces<<<grid_for(faces), kThreads, 0, s>>>(nx, ny, nz, x_faces, y_faces,
+                                                    z_faces, neumann, beta, fx, fy,
+                                                    fz);
+  k_beta_diagonal<<<grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0,
+                    s>>>(nx, ny, nz, fx, fy, fz, storage, diag);
+}
+void launch_shortcut_ratio(cudaStream_t s, const Level<double>& L,
+                           Reduce red) {
+  k_shortcut_ratio<<<reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s>>>(L, red);
+}
+template <class TO, class TI>
+void launch_convert(cudaStream_t s, size_t n, const TI* src, TO* dst) {
+  k_convert<TO, TI><<<grid_for(static_cast<long long>(n)), kThreads, 0, s>>>(n, src,
+                                                                           dst);
+}
+void launch_face_gradients(cudaStream_t s, const Level<double>& L,
+                           const double* lambda, const double* p,
+                           const double* fx_in, const double* fy_in,
+                           const double* fz_in, double* gx, double* gy,
+                           double* gz) {
+  (void)fx_in;
+  (void)fy_in;
+  (void)fz_in;
+  const long long faces = static_cast<long long>(L.nx + 1) * L.ny * L.nz +
+                          static_cast<long long>(L.nx) * (L.ny + 1) * L.nz +
+                          static_cast<long long>(L.nx) * L.ny * (L.nz + 1);
+  k_face_gradients<<<grid_for(faces), kThreads, 0, s>>>(L, lambda, p, gx, gy, gz);
+}
+void launch_adjoint_source(cudaStream_t s, int n, const double* dl_dp,
+                           const uint8_t* active, double* out) {
+  k_adjoint_source<<<grid_for(n), kThreads, 0, s>>>(n, dl_dp, active, out);
+}
+
+#define HFPS_INSTANTIATE(T)                                                        \
+  template void launch_level_apply<T>(cudaStream_t, const Level<T>&, const T*, T*); \
+  template void launch_level_defect<T>(cudaStream_t, const Level<T>&, const T*,    \
+                                       const T*, T*);                              \
+  template void launch_rb_color<T>(cudaStream_t, const Level<T>&, T*, const T*,    \
+                                   int);                                           \
+  template void launch_chebyshev_stage<T>(cudaStream_t, const Level<T>&, const T*, \
+                                          const T*, T*, T*, T, T, int);            \
+  template void launch_defect_restrict<T>(cudaStream_t, const Level<T>&, const T*, \
+                                          const T*, const Level<T>&, T*, T*, int); \
+  template void launch_restrict<T>(cudaStream_t, const Level<T>&, const T*,        \
+                                   const Level<T>&, T*, T*, int);                  \
+  template void launch_prolongate<T>(cudaStream_t, const Level<T>&, T*,            \
+                                     const Level<T>&, const T*, int);              \
+  template void launch_mg_enter<T>(cudaStream_t, int, const double*,               \
+                                   const uint8_t*, T*, T*);                        \
+  template void launch_mg_exit<T>(cudaStream_t, int, const T*, const uint8_t*,     \
+                                  const double*, double*);                         \
+  template void launch_diagonal_solve<T>(cudaStream_t, int, const T*, const T*,    \
+                                         T*);                                      \
+  template void launch_mg_projection<T>(cudaStream_t, int, const double*,          \
+                                        const uint8_t*, const T*, Reduce);
+
+HFPS_INSTANTIATE(double)
+HFPS_INSTANTIATE(float)
+
+template void launch_coarse_solve<double, double>(cudaStream_t, const Level<double>&,
+                                                  double*, const double*, double*,
+                                                  double*, double*, double*, int, int);
+template void launch_coarse_solve<float, double>(cudaStream_t, const Level<double>&,
+                                                 float*, const float*, double*,
+                                                 double*, double*, double*, int, int);
+template void launch_convert<float, double>(cudaStream_t, size_t, const double*, float*);
+template void launch_convert<double, float>(cudaStream_t, size_t, const float*, double*);
+
+}  // namespace hfps

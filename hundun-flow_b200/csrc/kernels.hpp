@@ -1,0 +1,171 @@
+// Host-callable launchers for the sm_100a kernels (kernels.cu).
+//
+// Every launcher enqueues on the given stream and never synchronises.  Level
+// operands are passed as hfps::Level<T> (hfps_device.cuh); vectors are dense
+// x-fastest arrays of the level's shape.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hfps_device.cuh"
+
+namespace hfps {
+
+// Device-resident Krylov scalars.  Kernels read alpha/beta from here, so a
+// whole iteration runs without a host round trip; the host reads back only
+// what steers control flow.
+struct Scalars {
+  double rho;        // r.z of the current search direction
+  double pap;        // p.Ap
+  double alpha;      // rho / pap
+  double rr;         // last r.r (recursive or true residual)
+  double rho_next;   // r.z after the preconditioner
+  double beta;       // rho_next / rho (0 after a restart)
+  double proj[3];    // MG projection sums r.r, r.Az, Az.Az
+  double mg_alpha;   // MG correction scale
+  double misc[4];
+  int flags;         // bit 0 non-finite, bit 1 breakdown
+  unsigned counters[8];  // last-block arrival counters, one per reduction
+};
+
+enum ScalarOp : int {
+  kOpPap = 0,        // pap = sum; alpha = rho / pap
+  kOpRecursive = 1,  // rr = sum
+  kOpRhoNext = 2,    // rho_next = sum; beta = rho_next / rho; rho = rho_next
+  kOpRhoRestart = 3, // rho = sum; beta = 0
+  kOpMisc = 4,       // misc[0] = sum
+};
+
+struct Reduce {
+  Scalars* scalars;
+  double* partials;   // >= gridDim.x * 3 doubles
+  int op;
+};
+
+int reduction_blocks(long long items);
+
+// ---- level operators (T = double or float) -------------------------------
+template <class T>
+void launch_level_apply(cudaStream_t s, const Level<T>& L, const T* x, T* y);
+template <class T>
+void launch_level_defect(cudaStream_t s, const Level<T>& L, const T* x,
+                         const T* b, T* r);
+template <class T>
+void launch_rb_color(cudaStream_t s, const Level<T>& L, T* x, const T* b,
+                     int color);
+template <class T>
+void launch_chebyshev_stage(cudaStream_t s, const Level<T>& L, const T* x,
+                            const T* b, T* direction, T* next,
+                            T previous_factor, T residual_factor, int first);
+template <class T>
+void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
+                            const T* b, const Level<T>& C, T* cb, T* cx,
+                            int coarsen_mask);
+template <class T>
+void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
+                     const Level<T>& C, T* cb, T* cx, int coarsen_mask);
+template <class T>
+void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
+                       const Level<T>& C, const T* cx, int coarsen_mask);
+// ---- zebra line relaxation (kernels_line.cu) --------------------------------
+// Line-colour passes with more lines than this run one Thomas recurrence per
+// thread; fewer lines run PCR with one CTA row per line.
+constexpr long long kLinePcrThreshold = 4096;
+enum LineKind : int { kLineNone = 0, kLineThomas = 1, kLinePcr = 2 };
+int line_kind(int nx, int ny, int nz, int axis);
+// Values of the factor block of one level and line axis: Thomas c' and
+// denominators (2 per cell) or PCR multipliers and final diagonals.
+size_t line_factor_values(int nx, int ny, int nz, int axis);
+template <class T>
+void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac);
+// One zebra colour; `scratch` holds the Thomas d' values (cells).
+template <class T>
+void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
+                      const T* fac, T* scratch, int axis, int color);
+// Coarsest level in line mode with x/rhs resident in shared memory; returns
+// false when the level is too large for that form.
+template <class T, class TC>
+bool launch_coarse_line(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
+                        const TC* fac, int sweeps, int axis);
+
+// Coarsest level: `sweeps` smoother sweeps in one CTA, arithmetic in TC.
+// Line mode when line_axis >= 0 (zebra line Gauss-Seidel).
+template <class T, class TC>
+void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
+                         TC* xs, TC* bs, TC* work, TC* dprime, int sweeps,
+                         int line_axis);
+
+// ---- MG entry/exit ------------------------------------------------------
+// b = active ? r : 0 (converted to T), x = 0.
+template <class T>
+void launch_mg_enter(cudaStream_t s, int n, const double* r,
+                     const uint8_t* active, T* b, T* x);
+// z = active ? x * scale : 0 (scale read from device when scale_ptr).
+template <class T>
+void launch_mg_exit(cudaStream_t s, int n, const T* x, const uint8_t* active,
+                    const double* scale_ptr, double* z);
+template <class T>
+void launch_diagonal_solve(cudaStream_t s, int n, const T* b, const T* diag,
+                           T* x);
+// Projection sums for the residual-minimising MG scale (level-0, FP64 r).
+template <class T>
+void launch_mg_projection(cudaStream_t s, int n, const double* r,
+                          const uint8_t* active, const T* recursive,
+                          Reduce red);
+
+// ---- Krylov (FP64) --------------------------------------------------------
+void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
+                     double* y, Reduce red);
+void launch_residual_norm(cudaStream_t s, const Level<double>& L,
+                          const double* x, const double* b, double* r,
+                          Reduce red);
+void launch_pcg_update(cudaStream_t s, int n, double* x, const double* p,
+                       double* r, const double* ap, Reduce red);
+void launch_dot(cudaStream_t s, int n, const double* a, const double* b,
+                Reduce red);
+void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
+                     const Scalars* sc);
+void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red);
+void launch_copy(cudaStream_t s, int n, const double* src, double* dst);
+
+// ---- setup (FP64) ---------------------------------------------------------
+void launch_mask_finest(cudaStream_t s, int nx, int ny, int nz,
+                        const double* x_faces, const double* y_faces,
+                        const double* z_faces, const double* diag_in,
+                        const double* fx_in, const double* fy_in,
+                        const double* fz_in, const uint8_t* active,
+                        double* diag, double* fx, double* fy, double* fz,
+                        double* volume, uint8_t* fluid);
+void launch_reaction(cudaStream_t s, const Level<double>& L,
+                     const double* volume, double* reaction);
+// One axis of the tensor aggregation (aggregate_tensor_channel).
+void launch_aggregate_axis(cudaStream_t s, const double* src, int ex, int ey,
+                           int ez, double* dst, int dx, int dy, int dz,
+                           int axis, int face_axis, int global_extent);
+void launch_coarse_diagonal(cudaStream_t s, int nx, int ny, int nz,
+                            double* diag, const double* fx, const double* fy,
+                            const double* fz, const double* volume,
+                            uint8_t* fluid);
+void launch_beta_coefficients(cudaStream_t s, int nx, int ny, int nz,
+                              const double* x_faces, const double* y_faces,
+                              const double* z_faces, unsigned neumann,
+                              const double* beta, const double* storage,
+                              double* diag, double* fx, double* fy,
+                              double* fz);
+void launch_shortcut_ratio(cudaStream_t s, const Level<double>& L,
+                           Reduce red);
+template <class TO, class TI>
+void launch_convert(cudaStream_t s, size_t n, const TI* src, TO* dst);
+
+// ---- adjoint ---------------------------------------------------------------
+void launch_face_gradients(cudaStream_t s, const Level<double>& L,
+                           const double* lambda, const double* p,
+                           const double* fx_in, const double* fy_in,
+                           const double* fz_in, double* gx, double* gy,
+                           double* gz);
+void launch_adjoint_source(cudaStream_t s, int n, const double* dl_dp,
+                           const uint8_t* active, double* out);
+
+}  // namespace hfps

@@ -1,0 +1,1029 @@
+// Host orchestration of the B200 pressure solve.  See solver.hpp.
+#include "solver.hpp"
+
+#include <algorithm>
+#include <cstdint>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <type_traits>
+
+namespace hfps {
+namespace {
+
+constexpr int kMaxLevels = 32;
+constexpr uint32_t kDetailPlan = 9101U;
+constexpr uint32_t kDetailCuda = 9102U;
+constexpr uint32_t kDetailNumeric = 9103U;
+constexpr uint32_t kDetailBreakdown = 9104U;
+
+size_t align_up(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
+
+struct Shape {
+  int n[3];
+  int coarsen_mask;
+  int line_mask;
+};
+
+// strategy_mask (src/solver_mg_workspace.cpp:113-143).
+int strategy_mask(const std::vector<double> (&faces)[3], double threshold,
+                  int& line_mask) {
+  double mn[3], mx[3], rep[3];
+  for (int a = 0; a < 3; ++a) {
+    mn[a] = std::numeric_limits<double>::infinity();
+    mx[a] = 0.0;
+    rep[a] = 0.0;
+    const int n = static_cast<int>(faces[a].size()) - 1;
+    for (int c = 0; c < n; ++c) {
+      const double w = faces[a][c + 1] - faces[a][c];
+      mn[a] = std::min(mn[a], w);
+      mx[a] = std::max(mx[a], w);
+      rep[a] += w;
+    }
+    rep[a] /= static_cast<double>(n);
+  }
+  const double largest = std::max({rep[0], rep[1], rep[2]});
+  line_mask = 0;
+  for (int a = 0; a < 3; ++a) {
+    const bool internal = mn[a] > 0.0 && mx[a] / mn[a] >= threshold;
+    const bool cross = rep[a] > 0.0 && largest / rep[a] >= threshold;
+    if (internal || cross) line_mask |= 1 << a;
+  }
+  const int all = 7;
+  if ((line_mask & (line_mask - 1)) != 0) return all;
+  const int candidate = all & ~line_mask;
+  return candidate == 0 ? all : candidate;
+}
+
+// Level shapes (make_mg_workspace_requirements, src/solver_mg_workspace.cpp:
+// 368-409): ceil-half every preferred axis whose extent exceeds the minimum
+// coarse extent until no axis can coarsen.
+std::vector<Shape> level_shapes(const std::vector<double> (&faces)[3],
+                                const hfps_policy& policy) {
+  int line_mask = 0;
+  const int preferred = strategy_mask(faces, policy.anisotropy_threshold, line_mask);
+  int g[3] = {static_cast<int>(faces[0].size()) - 1,
+              static_cast<int>(faces[1].size()) - 1,
+              static_cast<int>(faces[2].size()) - 1};
+  std::vector<Shape> shapes;
+  for (int l = 0; l < policy.maximum_levels; ++l) {
+    Shape s{{g[0], g[1], g[2]}, 0, line_mask};
+    int next[3] = {g[0], g[1], g[2]};
+    for (int a = 0; a < 3; ++a) {
+      if ((preferred & (1 << a)) && g[a] > policy.minimum_coarse_extent) {
+        s.coarsen_mask |= 1 << a;
+        next[a] = (g[a] + 1) / 2;
+      }
+    }
+    shapes.push_back(s);
+    if (s.coarsen_mask == 0 || static_cast<int>(shapes.size()) == policy.maximum_levels)
+      break;
+    std::copy(next, next + 3, g);
+  }
+  return shapes;
+}
+
+bool valid_policy(const hfps_policy& p) {
+  return std::isfinite(p.anisotropy_threshold) && p.anisotropy_threshold > 1.0 &&
+         p.pre_sweeps > 0 && p.pre_sweeps <= 255 && p.post_sweeps > 0 &&
+         p.post_sweeps <= 255 && p.maximum_levels >= 2 &&
+         p.maximum_levels <= kMaxLevels && p.coarse_sweeps > 0 &&
+         p.coarse_sweeps <= 65535 && p.minimum_coarse_extent >= 2 &&
+         (p.point_smoother == 0 || p.point_smoother == 1) &&
+         (p.cycle == 0 || p.cycle == 1) &&
+         std::isfinite(p.chebyshev_lower_spectrum_fraction) &&
+         p.chebyshev_lower_spectrum_fraction > 0.0 &&
+         p.chebyshev_lower_spectrum_fraction < 1.0 &&
+         std::isfinite(p.diagonal_shortcut_maximum_ratio) &&
+         p.diagonal_shortcut_maximum_ratio >= 0.0 &&
+         p.diagonal_shortcut_maximum_ratio < 1.0 &&
+         (p.unit_linear == 0 || p.unit_linear == 1);
+}
+
+}  // namespace
+
+Status Solver::fail(int code, uint32_t detail, const std::string& what) {
+  error_ = what;
+  return Status{code, detail};
+}
+
+Status Solver::check(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return {};
+  error_ = std::string(what) + ": " + cudaGetErrorString(e);
+  return Status{e == cudaErrorMemoryAllocation ? HFPS_ALLOCATION_FAILURE
+                                                : HFPS_INVALID_PLAN,
+                kDetailCuda};
+}
+
+Solver::~Solver() {
+  if (stream_ != nullptr) cudaStreamSynchronize(stream_);
+  for (auto& g : mg_graph_)
+    if (g != nullptr) cudaGraphExecDestroy(g);
+  if (h_scalars_ != nullptr) cudaFreeHost(h_scalars_);
+  if (arena_ != nullptr) cudaFree(arena_);
+  if (own_stream_ && stream_ != nullptr) cudaStreamDestroy(stream_);
+}
+
+Status Solver::create(const hfps_geometry& g, const hfps_policy& policy,
+                      cudaStream_t stream, Solver** out, std::string& error) {
+  *out = nullptr;
+  if (g.nx <= 0 || g.ny <= 0 || g.nz <= 0 || g.x_faces == nullptr ||
+      g.y_faces == nullptr || g.z_faces == nullptr || !valid_policy(policy)) {
+    error = "invalid geometry or policy";
+    return Status{HFPS_INVALID_PLAN, kDetailPlan};
+  }
+  const long long faces =
+      static_cast<long long>(g.nx + 1) * g.ny * g.nz +
+      static_cast<long long>(g.nx) * (g.ny + 1) * g.nz +
+      static_cast<long long>(g.nx) * g.ny * (g.nz + 1);
+  if (faces >= std::numeric_limits<int>::max()) {
+    error = "grid too large for 32-bit indexing";
+    return Status{HFPS_INVALID_PLAN, kDetailPlan};
+  }
+  unsigned neumann = 0;
+  for (int f = 0; f < 6; ++f) {
+    if (g.boundary[f] == HFPS_NEUMANN) neumann |= 1u << f;
+    else if (g.boundary[f] != HFPS_DIRICHLET) {
+      error = "periodic boundaries are not supported";
+      return Status{HFPS_INVALID_PLAN, kDetailPlan};
+    }
+  }
+  Solver* s = new Solver();
+  s->nx_ = g.nx;
+  s->ny_ = g.ny;
+  s->nz_ = g.nz;
+  s->neumann_ = neumann;
+  s->policy_ = policy;
+  const double* src[3] = {g.x_faces, g.y_faces, g.z_faces};
+  const int n[3] = {g.nx, g.ny, g.nz};
+  for (int a = 0; a < 3; ++a) {
+    s->faces_[a].assign(src[a], src[a] + n[a] + 1);
+    for (int c = 0; c < n[a]; ++c) {
+      if (!(s->faces_[a][c + 1] > s->faces_[a][c])) {
+        delete s;
+        error = "face coordinates must increase";
+        return Status{HFPS_INVALID_PLAN, kDetailPlan};
+      }
+    }
+  }
+  const size_t cells = static_cast<size_t>(g.nx) * g.ny * g.nz;
+  if (g.cell_active != nullptr) {
+    s->has_active_ = true;
+    s->active_host_.assign(g.cell_active, g.cell_active + cells);
+    for (uint8_t v : s->active_host_) {
+      if (v > 1) {
+        delete s;
+        error = "cell activity must be 0 or 1";
+        return Status{HFPS_INVALID_PLAN, kDetailPlan};
+      }
+    }
+  }
+  if (stream == nullptr) {
+    Status st = s->check(cudaStreamCreateWithFlags(&s->stream_, cudaStreamNonBlocking),
+                         "stream create");
+    if (!st) {
+      error = s->error_;
+      delete s;
+      return st;
+    }
+    s->own_stream_ = true;
+  } else {
+    s->stream_ = stream;
+  }
+  Status st = s->allocate();
+  if (!st) {
+    error = s->error_;
+    delete s;
+    return st;
+  }
+  *out = s;
+  return {};
+}
+
+Status Solver::allocate() {
+  const std::vector<Shape> shapes = level_shapes(faces_, policy_);
+  if (shapes.size() < 2) return fail(HFPS_INVALID_PLAN, kDetailPlan, "fewer than two levels");
+  const int levels = static_cast<int>(shapes.size());
+  // Sizes.
+  size_t bytes = 0;
+  const auto add = [&](size_t b) {
+    const size_t offset = bytes;
+    bytes += align_up(b);
+    return offset;
+  };
+  struct Offsets {
+    size_t d, fx, fy, fz, x, b, r, t, vol, fluid;
+    size_t d32, fx32, fy32, fz32, x32, b32, r32, t32;
+    size_t lf64[3], lf32[3];
+  };
+  std::vector<Offsets> off(levels);
+  size_t max_faces = 0;
+  for (int l = 0; l < levels; ++l) {
+    const Shape& s = shapes[l];
+    const size_t c = static_cast<size_t>(s.n[0]) * s.n[1] * s.n[2];
+    const size_t fx = static_cast<size_t>(s.n[0] + 1) * s.n[1] * s.n[2];
+    const size_t fy = static_cast<size_t>(s.n[0]) * (s.n[1] + 1) * s.n[2];
+    const size_t fz = static_cast<size_t>(s.n[0]) * s.n[1] * (s.n[2] + 1);
+    max_faces = std::max({max_faces, fx, fy, fz});
+    Offsets& o = off[l];
+    o.d = add(c * 8); o.fx = add(fx * 8); o.fy = add(fy * 8); o.fz = add(fz * 8);
+    o.x = add(c * 8); o.b = add(c * 8); o.r = add(c * 8); o.t = add(c * 8);
+    o.vol = add(c * 8); o.fluid = add(c);
+    o.d32 = add(c * 4); o.fx32 = add(fx * 4); o.fy32 = add(fy * 4); o.fz32 = add(fz * 4);
+    o.x32 = add(c * 4); o.b32 = add(c * 4); o.r32 = add(c * 4); o.t32 = add(c * 4);
+    for (int a = 0; a < 3; ++a) {
+      o.lf64[a] = o.lf32[a] = SIZE_MAX;
+      if (!(s.line_mask & (1 << a))) continue;
+      const size_t values = line_factor_values(s.n[0], s.n[1], s.n[2], a);
+      o.lf64[a] = add(values * 8);
+      o.lf32[a] = add(values * 4);
+    }
+  }
+  const size_t cells = static_cast<size_t>(nx_) * ny_ * nz_;
+  size_t faces_off[3];
+  faces_off[0] = add((nx_ + 1) * 8);
+  faces_off[1] = add((ny_ + 1) * 8);
+  faces_off[2] = add((nz_ + 1) * 8);
+  const size_t active_off = add(cells);
+  size_t agg_off[3];
+  for (auto& a : agg_off) a = add(max_faces * 8);
+  const size_t nfx = static_cast<size_t>(nx_ + 1) * ny_ * nz_;
+  const size_t nfy = static_cast<size_t>(nx_) * (ny_ + 1) * nz_;
+  const size_t nfz = static_cast<size_t>(nx_) * ny_ * (nz_ + 1);
+  size_t user_off[4];
+  user_off[0] = add(cells * 8);
+  user_off[1] = add(nfx * 8);
+  user_off[2] = add(nfy * 8);
+  user_off[3] = add(nfz * 8);
+  size_t k_off[6];
+  for (auto& k : k_off) k = add(cells * 8);
+  const size_t scalars_off = add(sizeof(Scalars));
+  const size_t partials_off = add(sizeof(double) * 3 * 148 * 8 + 4096);
+  arena_bytes_ = bytes;
+  Status st = check(cudaMalloc(&arena_, arena_bytes_), "device arena");
+  if (!st) return st;
+  st = check(cudaMemsetAsync(arena_, 0, arena_bytes_, stream_), "arena clear");
+  if (!st) return st;
+  st = check(cudaMallocHost(&h_scalars_, sizeof(Scalars)), "pinned scalars");
+  if (!st) return st;
+  std::memset(h_scalars_, 0, sizeof(Scalars));
+  const auto at = [&](size_t o) { return arena_ + o; };
+  for (int a = 0; a < 3; ++a) {
+    d_faces_[a] = reinterpret_cast<double*>(at(faces_off[a]));
+    st = check(cudaMemcpyAsync(d_faces_[a], faces_[a].data(),
+                               faces_[a].size() * sizeof(double),
+                               cudaMemcpyHostToDevice, stream_),
+               "faces upload");
+    if (!st) return st;
+  }
+  if (has_active_) {
+    d_active_ = reinterpret_cast<uint8_t*>(at(active_off));
+    st = check(cudaMemcpyAsync(d_active_, active_host_.data(), cells,
+                               cudaMemcpyHostToDevice, stream_),
+               "activity upload");
+    if (!st) return st;
+  }
+  for (auto a = 0; a < 3; ++a) agg_[a] = reinterpret_cast<double*>(at(agg_off[a]));
+  for (int u = 0; u < 4; ++u) user_[u] = reinterpret_cast<double*>(at(user_off[u]));
+  kx_ = reinterpret_cast<double*>(at(k_off[0]));
+  kr_ = reinterpret_cast<double*>(at(k_off[1]));
+  kz_ = reinterpret_cast<double*>(at(k_off[2]));
+  kp_ = reinterpret_cast<double*>(at(k_off[3]));
+  kap_ = reinterpret_cast<double*>(at(k_off[4]));
+  kb_ = reinterpret_cast<double*>(at(k_off[5]));
+  d_scalars_ = reinterpret_cast<Scalars*>(at(scalars_off));
+  d_partials_ = reinterpret_cast<double*>(at(partials_off));
+  l64_.resize(levels);
+  l32_.resize(levels);
+  volume_.resize(levels);
+  fluid_.resize(levels);
+  for (int l = 0; l < levels; ++l) {
+    const Shape& s = shapes[l];
+    const Offsets& o = off[l];
+    DeviceLevel<double>& a = l64_[l];
+    DeviceLevel<float>& b = l32_[l];
+    a.nx = b.nx = s.n[0];
+    a.ny = b.ny = s.n[1];
+    a.nz = b.nz = s.n[2];
+    a.coarsen_mask = b.coarsen_mask = s.coarsen_mask;
+    a.line_mask = b.line_mask = s.line_mask;
+    // build_levels: Chebyshev only on non-coarsest point levels
+    // (src/solver_mg.cpp:1060-1073).
+    a.chebyshev = b.chebyshev =
+        l + 1 < levels && s.line_mask == 0 && policy_.point_smoother == 1;
+    a.diag = reinterpret_cast<double*>(at(o.d));
+    a.fx = reinterpret_cast<double*>(at(o.fx));
+    a.fy = reinterpret_cast<double*>(at(o.fy));
+    a.fz = reinterpret_cast<double*>(at(o.fz));
+    a.x = reinterpret_cast<double*>(at(o.x));
+    a.b = reinterpret_cast<double*>(at(o.b));
+    a.r = reinterpret_cast<double*>(at(o.r));
+    a.t = reinterpret_cast<double*>(at(o.t));
+    volume_[l] = reinterpret_cast<double*>(at(o.vol));
+    fluid_[l] = reinterpret_cast<uint8_t*>(at(o.fluid));
+    a.fluid = b.fluid = fluid_[l];
+    b.diag = reinterpret_cast<float*>(at(o.d32));
+    b.fx = reinterpret_cast<float*>(at(o.fx32));
+    b.fy = reinterpret_cast<float*>(at(o.fy32));
+    b.fz = reinterpret_cast<float*>(at(o.fz32));
+    b.x = reinterpret_cast<float*>(at(o.x32));
+    b.b = reinterpret_cast<float*>(at(o.b32));
+    b.r = reinterpret_cast<float*>(at(o.r32));
+    b.t = reinterpret_cast<float*>(at(o.t32));
+    for (int ax = 0; ax < 3; ++ax) {
+      if (o.lf64[ax] == SIZE_MAX) continue;
+      a.lfac[ax] = reinterpret_cast<double*>(at(o.lf64[ax]));
+      b.lfac[ax] = reinterpret_cast<float*>(at(o.lf32[ax]));
+    }
+  }
+  return check(cudaStreamSynchronize(stream_), "allocation");
+}
+
+void Solver::level_shape(int level, int* out) const {
+  const DeviceLevel<double>& L = l64_[level];
+  out[0] = L.nx;
+  out[1] = L.ny;
+  out[2] = L.nz;
+  out[3] = L.line_mask;
+}
+
+Status Solver::copy_in(double* dst, const double* src, size_t n, int memory) {
+  return check(cudaMemcpyAsync(dst, src, n * sizeof(double),
+                               memory == HFPS_DEVICE ? cudaMemcpyDeviceToDevice
+                                                     : cudaMemcpyHostToDevice,
+                               stream_),
+               "copy in");
+}
+
+Status Solver::copy_out(double* dst, const double* src, size_t n, int memory) {
+  return check(cudaMemcpyAsync(dst, src, n * sizeof(double),
+                               memory == HFPS_DEVICE ? cudaMemcpyDeviceToDevice
+                                                     : cudaMemcpyDeviceToHost,
+                               stream_),
+               "copy out");
+}
+
+// One channel of aggregate_tensor_channel over the axes the fine level
+// coarsens, in x->y->z order (src/solver_mg.cpp:1706-1856).
+void Solver::aggregate_channel(int level, int face_axis, const double* src,
+                               double* dst) {
+  const DeviceLevel<double>& F = l64_[level];
+  int e[3] = {F.nx, F.ny, F.nz};
+  int g[3] = {F.nx, F.ny, F.nz};
+  if (face_axis >= 0) e[face_axis] += 1;
+  const double* cur = src;
+  int buffer = 0;
+  int remaining = 0;
+  for (int a = 0; a < 3; ++a)
+    if (F.coarsen_mask & (1 << a)) ++remaining;
+  for (int axis = 0; axis < 3; ++axis) {
+    if (!(F.coarsen_mask & (1 << axis))) continue;
+    --remaining;
+    int ng[3] = {g[0], g[1], g[2]};
+    ng[axis] = (g[axis] + 1) / 2;
+    int ne[3] = {ng[0], ng[1], ng[2]};
+    if (face_axis >= 0) ne[face_axis] += 1;
+    double* out = remaining == 0 ? dst : agg_[buffer];
+    launch_aggregate_axis(stream_, cur, e[0], e[1], e[2], out, ne[0], ne[1], ne[2],
+                          axis, face_axis, g[axis]);
+    cur = out;
+    buffer ^= 1;
+    std::copy(ng, ng + 3, g);
+    std::copy(ne, ne + 3, e);
+  }
+}
+
+Status Solver::build_hierarchy() {
+  for (size_t l = 1; l < l64_.size(); ++l) {
+    const DeviceLevel<double>& F = l64_[l - 1];
+    DeviceLevel<double>& C = l64_[l];
+    aggregate_channel(static_cast<int>(l - 1), -1, volume_[l - 1], volume_[l]);
+    launch_reaction(stream_, F.view(neumann_), volume_[l - 1], agg_[2]);
+    aggregate_channel(static_cast<int>(l - 1), -1, agg_[2], C.diag);
+    aggregate_channel(static_cast<int>(l - 1), 0, F.fx, C.fx);
+    aggregate_channel(static_cast<int>(l - 1), 1, F.fy, C.fy);
+    aggregate_channel(static_cast<int>(l - 1), 2, F.fz, C.fz);
+    launch_coarse_diagonal(stream_, C.nx, C.ny, C.nz, C.diag, C.fx, C.fy, C.fz,
+                           volume_[l], fluid_[l]);
+  }
+  for (auto& L : l64_)
+    for (int a = 0; a < 3; ++a)
+      if (L.lfac[a] != nullptr) launch_line_factors<double>(stream_, L.view(neumann_), a, L.lfac[a]);
+  Status st = check(cudaGetLastError(), "hierarchy kernels");
+  if (!st) return st;
+  // Diagonal shortcut (select_diagonal_shortcut, src/solver_mg.cpp:1577-1611).
+  diagonal_shortcut_ = false;
+  if (policy_.diagonal_shortcut_maximum_ratio != 0.0) {
+    const Level<double> L0 = l64_[0].view(neumann_);
+    launch_shortcut_ratio(stream_, L0, Reduce{d_scalars_, d_partials_, kOpMisc});
+    const int blocks = reduction_blocks(static_cast<long long>(L0.nx) * L0.ny * L0.nz);
+    std::vector<double> partial(blocks);
+    st = check(cudaMemcpyAsync(partial.data(), d_partials_, blocks * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "shortcut readback");
+    if (!st) return st;
+    st = check(cudaStreamSynchronize(stream_), "shortcut");
+    if (!st) return st;
+    double maximum = 0.0;
+    for (double v : partial) maximum = std::max(maximum, v);
+    diagonal_shortcut_ = maximum <= policy_.diagonal_shortcut_maximum_ratio;
+  }
+  // Validate the certified hierarchy: positive finite diagonals.
+  std::vector<double> probe;
+  for (size_t l = 0; l < l64_.size(); ++l) {
+    const DeviceLevel<double>& L = l64_[l];
+    if (L.cells() > (1 << 16)) continue;
+    probe.resize(L.cells());
+    st = check(cudaMemcpyAsync(probe.data(), L.diag, probe.size() * sizeof(double),
+                               cudaMemcpyDeviceToHost, stream_),
+               "diagonal probe");
+    if (!st) return st;
+    st = check(cudaStreamSynchronize(stream_), "diagonal probe");
+    if (!st) return st;
+    for (double d : probe)
+      if (!(d > 0.0) || !std::isfinite(d))
+        return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric,
+                    "non-positive coarse diagonal");
+  }
+  coefficients_ready_ = true;
+  mixed_ready_ = false;
+  for (auto& gexec : mg_graph_) {
+    if (gexec != nullptr) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+  }
+  return check(cudaStreamSynchronize(stream_), "hierarchy");
+}
+
+Status Solver::refresh_mixed() {
+  if (mixed_ready_) return {};
+  for (size_t l = 0; l < l64_.size(); ++l) {
+    const DeviceLevel<double>& a = l64_[l];
+    DeviceLevel<float>& b = l32_[l];
+    launch_convert<float, double>(stream_, a.cells(), a.diag, b.diag);
+    launch_convert<float, double>(stream_, a.faces_x(), a.fx, b.fx);
+    launch_convert<float, double>(stream_, a.faces_y(), a.fy, b.fy);
+    launch_convert<float, double>(stream_, a.faces_z(), a.fz, b.fz);
+  }
+  for (auto& L : l32_)
+    for (int a = 0; a < 3; ++a)
+      if (L.lfac[a] != nullptr) launch_line_factors<float>(stream_, L.view(neumann_), a, L.lfac[a]);
+  mixed_ready_ = true;
+  return check(cudaGetLastError(), "mixed conversion");
+}
+
+Status Solver::set_coefficients(const double* diag, const double* fx,
+                                const double* fy, const double* fz,
+                                int memory) {
+  if (diag == nullptr || fx == nullptr || fy == nullptr || fz == nullptr)
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "null coefficient array");
+  const size_t cells = static_cast<size_t>(nx_) * ny_ * nz_;
+  const size_t nf[3] = {static_cast<size_t>(nx_ + 1) * ny_ * nz_,
+                        static_cast<size_t>(nx_) * (ny_ + 1) * nz_,
+                        static_cast<size_t>(nx_) * ny_ * (nz_ + 1)};
+  if (memory == HFPS_HOST) {
+    // finite_coefficients (src/solver_mg.cpp:147-177): diagonal > 0, faces >= 0.
+    for (size_t c = 0; c < cells; ++c)
+      if (!(diag[c] > 0.0) || !std::isfinite(diag[c]))
+        return fail(HFPS_INVALID_PLAN, kDetailPlan, "diagonal must be positive and finite");
+    const double* f[3] = {fx, fy, fz};
+    for (int a = 0; a < 3; ++a)
+      for (size_t i = 0; i < nf[a]; ++i)
+        if (f[a][i] < 0.0 || !std::isfinite(f[a][i]))
+          return fail(HFPS_INVALID_PLAN, kDetailPlan, "face coefficients must be finite and >= 0");
+  }
+  Status st = copy_in(user_[0], diag, cells, memory);
+  if (st) st = copy_in(user_[1], fx, nf[0], memory);
+  if (st) st = copy_in(user_[2], fy, nf[1], memory);
+  if (st) st = copy_in(user_[3], fz, nf[2], memory);
+  if (!st) return st;
+  DeviceLevel<double>& L0 = l64_[0];
+  launch_mask_finest(stream_, nx_, ny_, nz_, d_faces_[0], d_faces_[1], d_faces_[2],
+                     user_[0], user_[1], user_[2], user_[3], d_active_, L0.diag,
+                     L0.fx, L0.fy, L0.fz, volume_[0], fluid_[0]);
+  return build_hierarchy();
+}
+
+Status Solver::set_beta(const double* beta, const double* storage, int memory) {
+  if (beta == nullptr) return fail(HFPS_INVALID_PLAN, kDetailPlan, "null beta");
+  const size_t cells = static_cast<size_t>(nx_) * ny_ * nz_;
+  Status st = copy_in(kz_, beta, cells, memory);
+  if (st && storage != nullptr) st = copy_in(kap_, storage, cells, memory);
+  if (!st) return st;
+  launch_beta_coefficients(stream_, nx_, ny_, nz_, d_faces_[0], d_faces_[1],
+                           d_faces_[2], neumann_, kz_,
+                           storage != nullptr ? kap_ : nullptr, user_[0], user_[1],
+                           user_[2], user_[3]);
+  DeviceLevel<double>& L0 = l64_[0];
+  launch_mask_finest(stream_, nx_, ny_, nz_, d_faces_[0], d_faces_[1], d_faces_[2],
+                     user_[0], user_[1], user_[2], user_[3], d_active_, L0.diag,
+                     L0.fx, L0.fy, L0.fz, volume_[0], fluid_[0]);
+  return build_hierarchy();
+}
+
+// ---------------------------------------------------------------------------
+// MG cycle (mg_cycle, src/solver_mg.cpp:4192-4338).
+
+template <class T>
+void Solver::smooth(std::vector<DeviceLevel<T>>& levels, int level, int sweeps,
+                    bool reverse) {
+  DeviceLevel<T>& L = levels[level];
+  const Level<T> view = L.view(neumann_);
+  if (L.line_mask == 0) {
+    if (L.chebyshev) {
+      // chebyshev_point_smooth_streamed (src/solver_mg.cpp:2916-3012): the
+      // ping-pong partner becomes the solution after odd stage counts.
+      constexpr double beta = 2.0;
+      const double alpha = policy_.chebyshev_lower_spectrum_fraction * beta;
+      const double theta = (beta + alpha) * 0.5;
+      const double delta = (beta - alpha) * 0.5;
+      const double sigma = theta / delta;
+      double previous_rho = 1.0 / sigma;
+      for (int s = 0; s < sweeps; ++s) {
+        const double rho = s == 0 ? 0.0 : 1.0 / (2.0 * sigma - previous_rho);
+        const double previous_factor = s == 0 ? 0.0 : rho * previous_rho;
+        const double residual_factor = s == 0 ? 1.0 / theta : 2.0 * rho / delta;
+        if (s != 0) previous_rho = rho;
+        launch_chebyshev_stage<T>(stream_, view, L.x, L.b, L.r, L.t,
+                                  static_cast<T>(previous_factor),
+                                  static_cast<T>(residual_factor), s == 0 ? 1 : 0);
+        std::swap(L.x, L.t);
+      }
+    } else {
+      const int first = reverse ? 1 : 0;
+      for (int s = 0; s < sweeps; ++s)
+        for (int pass = 0; pass < 2; ++pass)
+          launch_rb_color<T>(stream_, view, L.x, L.b, (first + pass) & 1);
+    }
+    return;
+  }
+  // smooth(): line relaxation along every strong axis, reversed on the way
+  // up (src/solver_mg.cpp:3566-3589); zebra colour order per sweep.
+  const auto run_axis = [&](int axis) {
+    const int first = reverse ? 1 : 0;
+    for (int s = 0; s < sweeps; ++s)
+      for (int pass = 0; pass < 2; ++pass)
+        launch_line_pass<T>(stream_, view, L.x, L.b, L.lfac[axis], L.r, axis,
+                            (first + pass) & 1);
+  };
+  if (reverse) {
+    for (int a = 3; a-- > 0;)
+      if (L.line_mask & (1 << a)) run_axis(a);
+  } else {
+    for (int a = 0; a < 3; ++a)
+      if (L.line_mask & (1 << a)) run_axis(a);
+  }
+}
+
+template <class T>
+void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels) {
+  DeviceLevel<T>& L = levels.back();
+  DeviceLevel<double>& D = l64_.back();
+  const Level<double> view = D.view(neumann_);
+  const bool widen = !std::is_same<T, double>::value;
+  double* xs = widen ? D.x : nullptr;
+  double* bs = widen ? D.b : nullptr;
+  if (L.line_mask == 0) {
+    launch_coarse_solve<T, double>(stream_, view, L.x, L.b, xs, bs, D.t, D.r,
+                                   policy_.coarse_sweeps, -1);
+    return;
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (!(L.line_mask & (1 << a))) continue;
+    if (!launch_coarse_line<T, double>(stream_, view, L.x, L.b, D.lfac[a],
+                                       policy_.coarse_sweeps, a))
+      launch_coarse_solve<T, double>(stream_, view, L.x, L.b, xs, bs, D.t, D.r,
+                                     policy_.coarse_sweeps, a);
+  }
+}
+
+template <class T>
+void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter) {
+  if (level + 1 == static_cast<int>(levels.size())) {
+    coarse_solve(levels);
+    return;
+  }
+  DeviceLevel<T>& F = levels[level];
+  DeviceLevel<T>& C = levels[level + 1];
+  smooth(levels, level, policy_.pre_sweeps, false);
+  // Retained defect + restrict_residual in one pass.
+  launch_defect_restrict<T>(stream_, F.view(neumann_), F.x, F.b, C.view(neumann_),
+                            C.b, C.x, F.coarsen_mask);
+  cycle(levels, level + 1, counter);
+  if (counter > 1) cycle(levels, level + 1, counter - 1);
+  launch_prolongate<T>(stream_, F.view(neumann_), F.x, C.view(neumann_), C.x,
+                       F.coarsen_mask);
+  smooth(levels, level, policy_.post_sweeps, true);
+}
+
+// NativeCartesianMgPlan::apply_impl (src/solver_mg.cpp:4814-5122).
+template <class T>
+void Solver::mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
+                        double* z) {
+  // Canonical buffer roles at entry, so captured and eager runs agree.
+  std::vector<std::pair<T*, T*>> saved;
+  for (auto& L : levels) saved.emplace_back(L.x, L.t);
+  DeviceLevel<T>& L0 = levels[0];
+  const int n = L0.cells();
+  launch_mg_enter<T>(stream_, n, r, d_active_, L0.b, L0.x);
+  if (diagonal_shortcut_) {
+    launch_diagonal_solve<T>(stream_, n, L0.b, L0.diag, L0.x);
+  } else {
+    cycle(levels, 0, policy_.cycle == 1 ? 2 : 1);
+  }
+  if (policy_.unit_linear) {
+    launch_mg_exit<T>(stream_, n, L0.x, d_active_, nullptr, z);
+  } else {
+    launch_level_defect<T>(stream_, L0.view(neumann_), L0.x, L0.b, L0.r);
+    launch_mg_projection<T>(stream_, n, r, d_active_, L0.r,
+                            Reduce{d_scalars_, d_partials_, 5});
+    launch_mg_exit<T>(stream_, n, L0.x, d_active_, &d_scalars_->mg_alpha, z);
+  }
+  for (size_t l = 0; l < levels.size(); ++l) {
+    levels[l].x = saved[l].first;
+    levels[l].t = saved[l].second;
+  }
+}
+
+Status Solver::mg_apply(bool mixed) {
+  if (mixed) {
+    Status st = refresh_mixed();
+    if (!st) return st;
+  }
+  const int slot = mixed ? 1 : 0;
+  if (!use_graphs_) {
+    if (mixed) mg_enqueue(l32_, kr_, kz_);
+    else mg_enqueue(l64_, kr_, kz_);
+    launches_ += mg_nodes_[slot];
+    return check(cudaGetLastError(), "mg launch");
+  }
+  if (mg_graph_[slot] == nullptr) {
+    cudaGraph_t graph = nullptr;
+    Status st = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal),
+                      "graph capture begin");
+    if (!st) return st;
+    if (mixed) mg_enqueue(l32_, kr_, kz_);
+    else mg_enqueue(l64_, kr_, kz_);
+    st = check(cudaStreamEndCapture(stream_, &graph), "graph capture end");
+    if (!st) return st;
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    mg_nodes_[slot] = nodes;
+    st = check(cudaGraphInstantiate(&mg_graph_[slot], graph, 0), "graph instantiate");
+    cudaGraphDestroy(graph);
+    if (!st) return st;
+  }
+  launches_ += mg_nodes_[slot];
+  return check(cudaGraphLaunch(mg_graph_[slot], stream_), "graph launch");
+}
+
+Status Solver::sync_scalars() {
+  Status st = check(cudaMemcpyAsync(h_scalars_, d_scalars_, sizeof(Scalars),
+                                    cudaMemcpyDeviceToHost, stream_),
+                    "scalar readback");
+  if (!st) return st;
+  return check(cudaStreamSynchronize(stream_), "solver step");
+}
+
+// solve_pcg (src/solver_krylov.cpp:1299-1555) with identical control flow:
+// true residual every `true_residual_interval` iterations, at a recursive
+// convergence claim and at the cap, and a restart of the search direction
+// (p = z) after every verification.
+Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
+                          double* history, uint32_t capacity) {
+  const int n = nx_ * ny_ * nz_;
+  const bool mixed = control.precision == HFPS_MIXED;
+  const Level<double> A = l64_[0].view(neumann_);
+  const auto red = [&](int op) { return Reduce{d_scalars_, d_partials_, op}; };
+  Status st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  launch_norm2(stream_, n, kb_, red(kOpMisc));
+  launches_ += 1;
+  st = sync_scalars();
+  if (!st) return st;
+  if (h_scalars_->flags & 1) {
+    result.termination = HFPS_NON_FINITE;
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite rhs");
+  }
+  const double bnorm = std::sqrt(h_scalars_->misc[0]);
+  const double tol = std::max(control.absolute_tolerance,
+                              control.relative_tolerance * bnorm);
+  result.rhs_norm = bnorm;
+  result.true_residual_limit = tol;
+  if (bnorm == 0.0) {
+    st = check(cudaMemsetAsync(kx_, 0, n * sizeof(double), stream_), "zero x");
+    result.termination = HFPS_ZERO_RHS;
+    return st;
+  }
+  launch_residual_norm(stream_, A, kx_, kb_, kr_, red(kOpRecursive));
+  launches_ += 1;
+  ++result.operator_applies;
+  st = sync_scalars();
+  if (!st) return st;
+  result.initial_true_residual = std::sqrt(h_scalars_->rr);
+  result.final_true_residual = result.initial_true_residual;
+  result.recursive_residual = result.initial_true_residual;
+  if (!std::isfinite(result.initial_true_residual)) {
+    result.termination = HFPS_NON_FINITE;
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite residual");
+  }
+  if (result.initial_true_residual <= tol) {
+    result.termination = HFPS_CONVERGED;
+    return {};
+  }
+  const auto restart_direction = [&]() -> Status {
+    Status s = mg_apply(mixed);
+    if (!s) return s;
+    ++result.preconditioner_applies;
+    launch_dot(stream_, n, kr_, kz_, red(kOpRhoRestart));
+    launch_copy(stream_, n, kz_, kp_);
+    launches_ += 2;
+    return {};
+  };
+  st = restart_direction();
+  if (!st) return st;
+  uint32_t it = 0;
+  while (it < control.maximum_iterations) {
+    launch_spmv_dot(stream_, A, kp_, kap_, red(kOpPap));
+    ++result.operator_applies;
+    launch_pcg_update(stream_, n, kx_, kp_, kr_, kap_, red(kOpRecursive));
+    launches_ += 2;
+    ++it;
+    st = sync_scalars();
+    if (!st) return st;
+    result.iterations = it;
+    // A breakdown flag comes from p.Ap of this iteration (the reference
+    // stops before counting it) or from the r.z that formed this direction
+    // (counted in the previous iteration): either way the reference reports
+    // one iteration fewer than this loop has taken.
+    if (h_scalars_->flags & 2) {
+      result.iterations = it - 1;
+      result.termination = HFPS_BREAKDOWN;
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailBreakdown, "Krylov breakdown");
+    }
+    if (h_scalars_->flags & 1) {
+      result.termination = HFPS_NON_FINITE;
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite Krylov scalar");
+    }
+    const double recursive = std::sqrt(h_scalars_->rr);
+    result.recursive_residual = recursive;
+    if (history != nullptr && it - 1 < capacity) {
+      history[it - 1] = recursive;
+      result.history_length = it;
+    }
+    const bool verify = recursive <= tol ||
+                        it % control.true_residual_interval == 0 ||
+                        it == control.maximum_iterations;
+    if (verify) {
+      launch_residual_norm(stream_, A, kx_, kb_, kr_, red(kOpRecursive));
+      launches_ += 1;
+      ++result.operator_applies;
+      st = sync_scalars();
+      if (!st) return st;
+      result.final_true_residual = std::sqrt(h_scalars_->rr);
+      result.recursive_residual = result.final_true_residual;
+      if (result.final_true_residual <= tol) {
+        result.termination = HFPS_CONVERGED;
+        return {};
+      }
+      if (it == control.maximum_iterations) break;
+      st = restart_direction();
+      if (!st) return st;
+      continue;
+    }
+    st = mg_apply(mixed);
+    if (!st) return st;
+    ++result.preconditioner_applies;
+    launch_dot(stream_, n, kr_, kz_, red(kOpRhoNext));
+    launch_p_update(stream_, n, kp_, kz_, d_scalars_);
+    launches_ += 2;
+  }
+  result.termination = HFPS_MAXIMUM_ITERATIONS;
+  return fail(HFPS_REJECTED_STEP, kDetailBreakdown, "maximum iterations reached");
+}
+
+Status Solver::solve(const double* rhs, double* solution, int memory,
+                     const hfps_control& control, hfps_result& result,
+                     double* history, uint32_t capacity) {
+  const auto begin = std::chrono::steady_clock::now();
+  result = hfps_result{};
+  result.levels = static_cast<uint32_t>(l64_.size());
+  result.termination = HFPS_TERMINATION_INVALID_PLAN;
+  if (!coefficients_ready_)
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "coefficients not set");
+  if (rhs == nullptr || solution == nullptr || control.maximum_iterations == 0 ||
+      control.true_residual_interval == 0 ||
+      !std::isfinite(control.relative_tolerance) ||
+      !std::isfinite(control.absolute_tolerance) ||
+      control.relative_tolerance < 0.0 || control.absolute_tolerance < 0.0 ||
+      (control.relative_tolerance == 0.0 && control.absolute_tolerance == 0.0) ||
+      control.algorithm != HFPS_PCG ||
+      (control.precision != HFPS_FP64 && control.precision != HFPS_MIXED) ||
+      control.restart != 0 || !policy_.unit_linear)
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "invalid solve control");
+  const size_t n = static_cast<size_t>(nx_) * ny_ * nz_;
+  Status st = copy_in(kb_, rhs, n, memory);
+  if (st) st = copy_in(kx_, solution, n, memory);
+  if (!st) return st;
+  launches_ = 0;
+  st = krylov_pcg(control, result, history, capacity);
+  result.kernel_launches = launches_;
+  if (st) {
+    st = copy_out(solution, kx_, n, memory);
+    if (st) st = check(cudaStreamSynchronize(stream_), "solution copy");
+  }
+  result.status = st.code;
+  result.detail = st.detail;
+  result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+  return st;
+}
+
+Status Solver::apply_operator(const double* x, double* y, int memory) {
+  if (!coefficients_ready_) return fail(HFPS_INVALID_PLAN, kDetailPlan, "coefficients not set");
+  const size_t n = static_cast<size_t>(nx_) * ny_ * nz_;
+  Status st = copy_in(kp_, x, n, memory);
+  if (!st) return st;
+  launch_level_apply<double>(stream_, l64_[0].view(neumann_), kp_, kap_);
+  st = copy_out(y, kap_, n, memory);
+  if (!st) return st;
+  return check(cudaStreamSynchronize(stream_), "operator");
+}
+
+Status Solver::apply_preconditioner(const double* r, double* z, int memory,
+                                    int precision) {
+  if (!coefficients_ready_) return fail(HFPS_INVALID_PLAN, kDetailPlan, "coefficients not set");
+  const size_t n = static_cast<size_t>(nx_) * ny_ * nz_;
+  Status st = copy_in(kr_, r, n, memory);
+  if (!st) return st;
+  st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  st = mg_apply(precision == HFPS_MIXED);
+  if (!st) return st;
+  st = copy_out(z, kz_, n, memory);
+  if (!st) return st;
+  return check(cudaStreamSynchronize(stream_), "preconditioner");
+}
+
+Status Solver::adjoint(const double* solution, const double* dl_dp,
+                       double* lambda, double* gx, double* gy, double* gz,
+                       int memory, const hfps_control& control,
+                       hfps_result& result) {
+  if (!coefficients_ready_) return fail(HFPS_INVALID_PLAN, kDetailPlan, "coefficients not set");
+  if (solution == nullptr || dl_dp == nullptr)
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "null adjoint input");
+  const size_t n = static_cast<size_t>(nx_) * ny_ * nz_;
+  // A is symmetric (SPD operator class, src/solver_ibm_pressure.cpp:242-245),
+  // so A^T lambda = dL/dp is the forward solve with rhs dL/dp masked to the
+  // fluid rows (solid rows are identities with zero rhs).
+  Status st = copy_in(kz_, dl_dp, n, memory);
+  if (!st) return st;
+  launch_adjoint_source(stream_, static_cast<int>(n), kz_, d_active_, kb_);
+  st = check(cudaMemsetAsync(kx_, 0, n * sizeof(double), stream_), "lambda init");
+  if (!st) return st;
+  const auto begin = std::chrono::steady_clock::now();
+  result = hfps_result{};
+  result.levels = static_cast<uint32_t>(l64_.size());
+  launches_ = 0;
+  st = krylov_pcg(control, result, nullptr, 0);
+  result.kernel_launches = launches_ + 1;
+  result.status = st.code;
+  result.detail = st.detail;
+  if (!st) return st;
+  // lambda now in kx_; p into kp_ (device copy of the forward solution).
+  st = copy_in(kp_, solution, n, memory);
+  if (!st) return st;
+  const DeviceLevel<double>& L0 = l64_[0];
+  const size_t nf[3] = {static_cast<size_t>(L0.faces_x()), static_cast<size_t>(L0.faces_y()),
+                        static_cast<size_t>(L0.faces_z())};
+  // Gradient staging: reuse the user coefficient staging buffers.
+  launch_face_gradients(stream_, L0.view(neumann_), kx_, kp_, nullptr, nullptr, nullptr,
+                        user_[1], user_[2], user_[3]);
+  if (lambda != nullptr) st = copy_out(lambda, kx_, n, memory);
+  if (st && gx != nullptr) st = copy_out(gx, user_[1], nf[0], memory);
+  if (st && gy != nullptr) st = copy_out(gy, user_[2], nf[1], memory);
+  if (st && gz != nullptr) st = copy_out(gz, user_[3], nf[2], memory);
+  if (st) st = check(cudaStreamSynchronize(stream_), "adjoint");
+  result.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - begin).count();
+  return st;
+}
+
+Status Solver::level_coefficients(int level, double* diag, double* fx,
+                                  double* fy, double* fz, double* volume) {
+  if (level < 0 || level >= level_count())
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "level out of range");
+  const DeviceLevel<double>& L = l64_[level];
+  Status st{};
+  if (diag) st = copy_out(diag, L.diag, L.cells(), HFPS_HOST);
+  if (st && fx) st = copy_out(fx, L.fx, L.faces_x(), HFPS_HOST);
+  if (st && fy) st = copy_out(fy, L.fy, L.faces_y(), HFPS_HOST);
+  if (st && fz) st = copy_out(fz, L.fz, L.faces_z(), HFPS_HOST);
+  if (st && volume) st = copy_out(volume, volume_[level], L.cells(), HFPS_HOST);
+  if (!st) return st;
+  return check(cudaStreamSynchronize(stream_), "level coefficients");
+}
+
+}  // namespace hfps
+
+namespace hfps {
+
+// Algorithmic bytes use w = sizeof(T) per cell-stream: stencil operand set
+// x, D, fx, fy, fz (5w), plus what each kernel writes or reads besides.
+Status Solver::profile_kernel(int kernel, int repetitions, double* ms,
+                              double* bytes) {
+  if (!coefficients_ready_) return fail(HFPS_INVALID_PLAN, kDetailPlan, "coefficients not set");
+  if (repetitions <= 0 || ms == nullptr || bytes == nullptr)
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "invalid profile request");
+  const int n = nx_ * ny_ * nz_;
+  const double cells = static_cast<double>(n);
+  DeviceLevel<double>& L0 = l64_[0];
+  DeviceLevel<float>& F0 = l32_[0];
+  const Level<double> A = L0.view(neumann_);
+  if (kernel == HFPS_KERNEL_SMOOTH_FP32 || kernel == HFPS_KERNEL_MG_MIXED) {
+    Status st = refresh_mixed();
+    if (!st) return st;
+  }
+  const auto red = [&](int op) { return Reduce{d_scalars_, d_partials_, op}; };
+  Status st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  // Deterministic finite operands.
+  launch_copy(stream_, n, kb_, kr_);
+  launch_copy(stream_, n, kb_, kp_);
+  const auto level0_smoother = [&](auto& levels) -> double {
+    auto& L = levels[0];
+    using T = typename std::remove_reference<decltype(L)>::type::value_type;
+    const Level<T> view = L.view(neumann_);
+    if (L.line_mask != 0) {
+      int axis = 0;
+      while (!(L.line_mask & (1 << axis))) ++axis;
+      launch_line_pass<T>(stream_, view, L.x, L.b, L.lfac[axis], L.r, axis, 0);
+      return 28.0 / 8.0 * sizeof(T);
+    }
+    if (L.chebyshev) {
+      launch_chebyshev_stage<T>(stream_, view, L.x, L.b, L.r, L.t, T(0.5), T(0.5), 0);
+      return 72.0 / 8.0 * sizeof(T);
+    }
+    launch_rb_color<T>(stream_, view, L.x, L.b, 0);
+    return 28.0 / 8.0 * sizeof(T);
+  };
+  cudaEvent_t start, stop;
+  cudaEventCreate(&start);
+  cudaEventCreate(&stop);
+  double per_cell = 0.0;
+  const auto one = [&]() {
+    switch (kernel) {
+      case HFPS_KERNEL_OPERATOR:
+        launch_spmv_dot(stream_, A, kp_, kap_, red(kOpMisc));
+        per_cell = 48.0;
+        break;
+      case HFPS_KERNEL_SMOOTH_FP64:
+        per_cell = level0_smoother(l64_);
+        break;
+      case HFPS_KERNEL_SMOOTH_FP32:
+        per_cell = level0_smoother(l32_);
+        break;
+      case HFPS_KERNEL_RESTRICT_FP64:
+        launch_defect_restrict<double>(stream_, A, L0.x, L0.b, l64_[1].view(neumann_),
+                                       l64_[1].b, l64_[1].x, L0.coarsen_mask);
+        per_cell = 48.0 + 2.0 * 8.0 / (l64_[0].cells() / static_cast<double>(l64_[1].cells()));
+        break;
+      case HFPS_KERNEL_PROLONG_FP64:
+        launch_prolongate<double>(stream_, A, L0.x, l64_[1].view(neumann_), l64_[1].x,
+                                  L0.coarsen_mask);
+        per_cell = 16.0 + 1.0 + 8.0 / (l64_[0].cells() / static_cast<double>(l64_[1].cells()));
+        break;
+      case HFPS_KERNEL_PCG_UPDATE:
+        launch_pcg_update(stream_, n, kx_, kp_, kr_, kap_, red(kOpMisc));
+        per_cell = 48.0;
+        break;
+      case HFPS_KERNEL_MG_FP64:
+      case HFPS_KERNEL_MG_MIXED:
+        mg_apply(kernel == HFPS_KERNEL_MG_MIXED);
+        per_cell = 0.0;
+        break;
+      default:
+        per_cell = -1.0;
+        break;
+    }
+  };
+  one();  // warm-up (also builds a graph when needed)
+  if (per_cell < 0.0) {
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "unknown kernel class");
+  }
+  cudaEventRecord(start, stream_);
+  for (int r = 0; r < repetitions; ++r) one();
+  cudaEventRecord(stop, stream_);
+  st = check(cudaEventSynchronize(stop), "profile");
+  float elapsed = 0.0f;
+  cudaEventElapsedTime(&elapsed, start, stop);
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  (void)F0;
+  if (!st) return st;
+  *ms = static_cast<double>(elapsed) / repetitions;
+  *bytes = per_cell * cells;
+  return check(cudaGetLastError(), "profile kernels");
+}
+
+}  // namespace hfps

@@ -1,0 +1,148 @@
+// Host side of the B200 pressure solve (C++17).
+//
+// One Solver owns the device hierarchy of one pressure system: the level
+// shapes (make_mg_workspace_requirements, src/solver_mg_workspace.cpp:
+// 317-452), the masked and aggregated level coefficients
+// (build_coarse_coefficients, src/solver_mg.cpp:1858-1925), the MG
+// workspaces and the Krylov vectors.  The MG cycle is orchestrated here and
+// captured once into a CUDA graph per precision; Krylov scalars stay on the
+// device, so an iteration costs one small device-to-host read.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/hf_pressure_solver.h"
+#include "kernels.hpp"
+
+namespace hfps {
+
+template <class T>
+struct DeviceLevel {
+  using value_type = T;
+  int nx{}, ny{}, nz{};
+  int coarsen_mask{};
+  int line_mask{};
+  bool chebyshev{};
+  T* diag{};
+  T* fx{};
+  T* fy{};
+  T* fz{};
+  const uint8_t* fluid{};
+  T* x{};
+  T* b{};
+  T* r{};
+  T* t{};
+  // Line-relaxation factors per strong axis (kernels_line.cu), or null.
+  T* lfac[3]{};
+  int cells() const { return nx * ny * nz; }
+  int faces_x() const { return (nx + 1) * ny * nz; }
+  int faces_y() const { return nx * (ny + 1) * nz; }
+  int faces_z() const { return nx * ny * (nz + 1); }
+  Level<T> view(unsigned neumann) const {
+    return Level<T>{nx, ny, nz, neumann, diag, fx, fy, fz, fluid};
+  }
+};
+
+struct Status {
+  int code{HFPS_OK};
+  uint32_t detail{};
+  explicit operator bool() const { return code == HFPS_OK; }
+};
+
+class Solver {
+ public:
+  ~Solver();
+  static Status create(const hfps_geometry& geometry, const hfps_policy& policy,
+                       cudaStream_t stream, Solver** out, std::string& error);
+
+  Status set_coefficients(const double* diag, const double* fx,
+                          const double* fy, const double* fz, int memory);
+  Status set_beta(const double* beta, const double* storage, int memory);
+  Status solve(const double* rhs, double* solution, int memory,
+               const hfps_control& control, hfps_result& result,
+               double* history, uint32_t history_capacity);
+  Status apply_operator(const double* x, double* y, int memory);
+  Status apply_preconditioner(const double* r, double* z, int memory,
+                              int precision);
+  Status adjoint(const double* solution, const double* dl_dp, double* lambda,
+                 double* gx, double* gy, double* gz, int memory,
+                 const hfps_control& control, hfps_result& result);
+  int level_count() const { return static_cast<int>(l64_.size()); }
+  void level_shape(int level, int* out) const;
+  Status level_coefficients(int level, double* diag, double* fx, double* fy,
+                            double* fz, double* volume);
+  Status profile_kernel(int kernel, int repetitions, double* ms,
+                        double* bytes);
+  const std::string& last_error() const { return error_; }
+
+ private:
+  Solver() = default;
+  Status fail(int code, uint32_t detail, const std::string& what);
+  Status check(cudaError_t e, const char* what);
+  Status allocate();
+  Status build_hierarchy();
+  Status refresh_mixed();
+  void aggregate_channel(int level, int face_axis, const double* src,
+                         double* dst);
+  // The MG preconditioner: z = M r on the internal r/z buffers.
+  Status mg_apply(bool mixed);
+  template <class T>
+  void mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
+                  double* z);
+  template <class T>
+  void cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter);
+  template <class T>
+  void smooth(std::vector<DeviceLevel<T>>& levels, int level, int sweeps,
+              bool reverse);
+  template <class T>
+  void coarse_solve(std::vector<DeviceLevel<T>>& levels);
+  Status krylov_pcg(const hfps_control& control, hfps_result& result,
+                    double* history, uint32_t capacity);
+  Status sync_scalars();
+  Status copy_in(double* dst, const double* src, size_t n, int memory);
+  Status copy_out(double* dst, const double* src, size_t n, int memory);
+
+  int nx_{}, ny_{}, nz_{};
+  unsigned neumann_{};
+  hfps_policy policy_{};
+  std::vector<double> faces_[3];
+  std::vector<uint8_t> active_host_;
+  bool has_active_{};
+  bool own_stream_{};
+  cudaStream_t stream_{};
+  std::string error_;
+
+  // Device storage: one arena for everything.
+  char* arena_{};
+  size_t arena_bytes_{};
+  double* d_faces_[3]{};
+  uint8_t* d_active_{};
+  std::vector<DeviceLevel<double>> l64_;
+  std::vector<DeviceLevel<float>> l32_;
+  std::vector<double*> volume_;
+  std::vector<uint8_t*> fluid_;
+  double* agg_[3]{};          // aggregation scratch (max face count each)
+  double* user_[4]{};         // staging for user coefficients (diag, fx, fy, fz)
+  double* kx_{};              // Krylov vectors
+  double* kr_{};
+  double* kz_{};
+  double* kp_{};
+  double* kap_{};
+  double* kb_{};
+  Scalars* d_scalars_{};
+  Scalars* h_scalars_{};      // pinned
+  double* d_partials_{};
+  bool coefficients_ready_{};
+  bool mixed_ready_{};
+  bool diagonal_shortcut_{};
+  cudaGraphExec_t mg_graph_[2]{};
+  size_t mg_nodes_[2]{};      // kernels per MG application (graph nodes)
+  uint64_t launches_{};       // kernels launched since the last reset
+  bool use_graphs_{true};
+};
+
+}  // namespace hfps

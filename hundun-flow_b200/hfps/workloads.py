@@ -262,6 +262,76 @@ def warm_start_rhs(system: PressureSystem, index: int, amplitude: float = 0.05) 
     return np.ascontiguousarray(system.rhs + extra)
 
 
+def _logical_shift(t, bits: int):
+    """Unsigned right shift of int64 tensors holding uint64 bit patterns."""
+    return (t >> bits) & ((1 << (64 - bits)) - 1)
+
+
+def _splitmix64_torch(counter):
+    import torch
+    golden = -7046029254386353131  # 0x9E3779B97F4A7C15 as int64
+    m1 = -4658895280553007687      # 0xBF58476D1CE4E5B9
+    m2 = -7723592293110705685      # 0x94D049BB133111EB
+    z = counter * golden + golden
+    z = (z ^ _logical_shift(z, 30)) * m1
+    z = (z ^ _logical_shift(z, 27)) * m2
+    return z ^ _logical_shift(z, 31)
+
+
+def normals_torch(seed: int, count: int, offset: int = 0, device="cuda"):
+    """Same stream as ``normals`` computed with torch int64 arithmetic
+    (two's-complement wrap-around equals uint64 arithmetic bit for bit)."""
+    import torch
+    base = (seed * 0x632BE59BD9B4E019 + 0x1234567) & 0xFFFFFFFFFFFFFFFF
+    if base >= 1 << 63:
+        base -= 1 << 64
+    index = torch.arange(offset, offset + count, dtype=torch.int64, device=device)
+    a = _splitmix64_torch(base + 2 * index)
+    b = _splitmix64_torch(base + 2 * index + 1)
+    u1 = (_logical_shift(a, 11).to(torch.float64) + 1.0) * (1.0 / 9007199254740992.0)
+    u2 = _logical_shift(b, 11).to(torch.float64) * (1.0 / 9007199254740992.0)
+    return torch.sqrt(-2.0 * torch.log(u1)) * torch.cos(2.0 * math.pi * u2)
+
+
+def flux_divergence_rhs_torch(seed: int, faces, boundary, active, scale: float = 1.0,
+                              device="cuda"):
+    """``flux_divergence_rhs`` on the GPU (same values up to the last ulp of
+    log/cos); returns a flat float64 CUDA tensor."""
+    import torch
+    nx, ny, nz = (len(f) - 1 for f in faces)
+    w = [torch.as_tensor(np.diff(f), dtype=torch.float64, device=device) for f in faces]
+    wx, wy, wz = w
+    n_x = (nx + 1) * ny * nz
+    n_y = nx * (ny + 1) * nz
+    n_z = nx * ny * (nz + 1)
+    u = normals_torch(seed, n_x + n_y + n_z, device=device)
+    ux = u[:n_x].reshape(nz, ny, nx + 1) * (wz[:, None, None] * wy[None, :, None])
+    uy = u[n_x:n_x + n_y].reshape(nz, ny + 1, nx) * (wz[:, None, None] * wx[None, None, :])
+    uz = u[n_x + n_y:].reshape(nz + 1, ny, nx) * (wy[None, :, None] * wx[None, None, :])
+    if active is not None:
+        ax, ay, az = (torch.as_tensor(t, device=device).to(torch.float64)
+                      for t in face_activity(active, (nx, ny, nz)))
+        ux, uy, uz = ux * ax, uy * ay, uz * az
+    if boundary[0] == NEUMANN:
+        ux[:, :, 0] = 0.0
+    if boundary[1] == NEUMANN:
+        ux[:, :, -1] = 0.0
+    if boundary[2] == NEUMANN:
+        uy[:, 0, :] = 0.0
+    if boundary[3] == NEUMANN:
+        uy[:, -1, :] = 0.0
+    if boundary[4] == NEUMANN:
+        uz[0, :, :] = 0.0
+    if boundary[5] == NEUMANN:
+        uz[-1, :, :] = 0.0
+    outward = (ux[:, :, 1:] - ux[:, :, :-1] + uy[:, 1:, :] - uy[:, :-1, :]
+               + uz[1:, :, :] - uz[:-1, :, :])
+    rhs = -scale * outward
+    if active is not None:
+        rhs = rhs * torch.as_tensor(active, device=device).to(torch.float64)
+    return rhs.reshape(-1).contiguous()
+
+
 CONFIGS = {
     # name: (builder, kwargs)
     "sphere64": (spherical_flame, dict(n=(64, 64, 64))),

@@ -1,0 +1,248 @@
+/*
+ * hf_pressure_solver.h -- C ABI of the B200 pressure-coupling linear solve.
+ *
+ * Drop-in for the reference's linear-solver/preconditioner interface on the
+ * cell-centred 7-point pressure system  div(beta grad p) = rhs  with IBM-
+ * masked cells.  Paths in the citations are relative to versions/v0.4 of the
+ * reference.  Every entry point returns an hfps_status whose values are the
+ * reference's StatusCode (include/hundun/v04_status.hpp:13-22); nothing
+ * throws across this boundary, and a failed solve publishes no solution
+ * (src/solver_krylov.cpp:1207-1250).
+ *
+ * Layout: every cell field is a dense x-fastest array of nx*ny*nz values;
+ * face arrays have extents (nx+1,ny,nz), (nx,ny+1,nz), (nx,ny,nz+1), also
+ * x-fastest (src/solver_mg.cpp:1456-1466).  A `memory` argument says whether
+ * the pointers are host memory (HFPS_HOST) or device memory on the solver's
+ * GPU (HFPS_DEVICE).  A handle is bound to one GPU and one CUDA stream and is
+ * not thread-safe, matching the reference's one-rank-one-thread contract.
+ */
+#ifndef HF_PRESSURE_SOLVER_H
+#define HF_PRESSURE_SOLVER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HFPS_API __attribute__((visibility("default")))
+#else
+#define HFPS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* StatusCode (include/hundun/v04_status.hpp:13-22). */
+typedef enum hfps_status {
+  HFPS_OK = 0,
+  HFPS_INVALID_CASE = 1,
+  HFPS_INVALID_PLAN = 2,
+  HFPS_ALLOCATION_FAILURE = 3,
+  HFPS_MPI_FAILURE = 4,
+  HFPS_NUMERICAL_FAILURE = 5,
+  HFPS_REJECTED_STEP = 6,
+  HFPS_IO_FAILURE = 7
+} hfps_status;
+
+/* LinearTermination (include/hundun/v04_linear.hpp:77-88). */
+typedef enum hfps_termination {
+  HFPS_CONVERGED = 0,
+  HFPS_ZERO_RHS = 1,
+  HFPS_MAXIMUM_ITERATIONS = 2,
+  HFPS_BREAKDOWN = 3,
+  HFPS_NON_FINITE = 4,
+  HFPS_OPERATOR_FAILURE = 5,
+  HFPS_PRECONDITIONER_FAILURE = 6,
+  HFPS_COLLECTIVE_FAILURE = 7,
+  HFPS_TERMINATION_INVALID_PLAN = 8
+} hfps_termination;
+
+/* MgBoundaryKind (include/hundun/v04_linear.hpp:100-104).  Periodic is
+ * rejected with HFPS_INVALID_PLAN. */
+typedef enum hfps_boundary {
+  HFPS_DIRICHLET = 0,
+  HFPS_NEUMANN = 1,
+  HFPS_PERIODIC = 2
+} hfps_boundary;
+
+typedef enum hfps_memory { HFPS_HOST = 0, HFPS_DEVICE = 1 } hfps_memory;
+
+/* LinearAlgorithm (include/hundun/v04_case.hpp:21). */
+typedef enum hfps_algorithm { HFPS_PCG = 0, HFPS_FGMRES = 1 } hfps_algorithm;
+
+/* FP64: every kernel in FP64.  MIXED: MG hierarchy stored and cycled in
+ * FP32 inside an FP64 Krylov/refinement loop; residuals, dot products, norms
+ * and the coarsest-grid solve stay FP64. */
+typedef enum hfps_precision { HFPS_FP64 = 0, HFPS_MIXED = 1 } hfps_precision;
+
+/* MgHierarchyPolicy (include/hundun/v04_linear.hpp:115-131) plus the
+ * correction scaling of NativeCartesianMgSpec (:316-329). */
+typedef struct hfps_policy {
+  int point_smoother;       /* 0 red-black (omega 0.72), 1 Chebyshev-Jacobi */
+  int cycle;                /* 0 V-cycle, 1 F-cycle */
+  int pre_sweeps;           /* default 2 */
+  int post_sweeps;          /* default 2 */
+  int coarse_sweeps;        /* default 24 */
+  int maximum_levels;       /* default 32 */
+  int minimum_coarse_extent;/* default 3 */
+  int unit_linear;          /* 1: correction scale 1 (fixed, PCG);
+                               0: residual-minimising (flexible, FGMRES) */
+  double chebyshev_lower_spectrum_fraction; /* default 0.3 */
+  double anisotropy_threshold;              /* default 4.0 */
+  double diagonal_shortcut_maximum_ratio;   /* default 0.0 (off) */
+} hfps_policy;
+
+/* Cartesian geometry: face coordinates per axis (n+1 values each),
+ * boundary kinds [x_min, x_max, y_min, y_max, z_min, z_max] and an optional
+ * host cell activity map (1 fluid, 0 IBM solid; NULL = all fluid). */
+typedef struct hfps_geometry {
+  int nx, ny, nz;
+  const double* x_faces;
+  const double* y_faces;
+  const double* z_faces;
+  int boundary[6];
+  const uint8_t* cell_active;
+} hfps_geometry;
+
+/* LinearSolveControl (include/hundun/v04_linear.hpp:453-465) plus the
+ * algorithm/precision selection. */
+typedef struct hfps_control {
+  double relative_tolerance;
+  double absolute_tolerance;
+  uint32_t maximum_iterations;
+  uint32_t true_residual_interval;
+  uint32_t restart;   /* FGMRES restart length; 0 for PCG */
+  int algorithm;      /* hfps_algorithm */
+  int precision;      /* hfps_precision */
+} hfps_control;
+
+/* LinearSolveResult subset (include/hundun/v04_linear.hpp:530-579). */
+typedef struct hfps_result {
+  int status;
+  uint32_t detail;
+  int termination;
+  uint32_t iterations;
+  double initial_true_residual;
+  double final_true_residual;
+  double recursive_residual;
+  double rhs_norm;
+  double true_residual_limit;
+  uint64_t operator_applies;
+  uint64_t preconditioner_applies;
+  uint32_t history_length;   /* entries written to the history buffer */
+  uint32_t levels;           /* MG levels in the hierarchy */
+  double seconds;            /* wall time of the solve on the host */
+  uint64_t kernel_launches;  /* this library's kernels launched by the call */
+} hfps_result;
+
+typedef struct hfps_solver hfps_solver;
+
+/* Fills `policy` with the MgHierarchyPolicy struct defaults (red-black
+ * V(2,2), 24 coarse sweeps, unit_linear). */
+HFPS_API void hfps_default_policy(hfps_policy* policy);
+/* production_pressure_mg_policy (src/solver_piso_detail.hpp:10-19):
+ * Chebyshev pre 1 / post 2, F-cycle, fraction 0.3, diagonal shortcut 0.1. */
+HFPS_API void hfps_production_policy(hfps_policy* policy);
+HFPS_API void hfps_default_control(hfps_control* control);
+
+/* Builds the level hierarchy and workspaces on the current CUDA device.
+ * Replaces NativeCartesianMgPlan::compile + make_mg_workspace_requirements +
+ * SolverWorkspace::bind (include/hundun/v04_linear.hpp:945-960, 1046-1064).
+ * `stream` is a cudaStream_t; NULL makes the solver create and own a
+ * non-blocking stream of its own. */
+HFPS_API int hfps_create(const hfps_geometry* geometry, const hfps_policy* policy,
+                void* stream, hfps_solver** out);
+
+/* Sets the operator: diagonal (cells) and face coefficients (unmasked, as
+ * the regular PressureLinearOperator receives them).  Solid cells become
+ * identity rows and every fluid/solid face is removed, exactly as
+ * IbmPressureOperator::decorate_pressure_action
+ * (src/solver_ibm_pressure.cpp:347-385) and copy_finest_coefficients
+ * (src/solver_mg.cpp:1469-1570) do; then the coarse levels are aggregated
+ * (build_coarse_coefficients, src/solver_mg.cpp:1858-1925).  Replaces
+ * NativeCartesianMgPlan::update_coefficients (v04_linear.hpp:955-960). */
+HFPS_API int hfps_set_coefficients(hfps_solver* solver, const double* diagonal,
+                          const double* face_x, const double* face_y,
+                          const double* face_z, int memory);
+
+/* Builds the coefficients from cell beta with face_pressure_coefficient's
+ * distance-weighted harmonic rule (src/solver_piso.cpp:1060-1136):
+ * interior c = A/(dL/bL + dR/bR), Dirichlet boundary c = A*b/d, Neumann 0;
+ * diagonal = sum of faces + storage (storage may be NULL). */
+HFPS_API int hfps_set_beta(hfps_solver* solver, const double* beta,
+                  const double* storage, int memory);
+
+/* solve(rhs, x0, tol) -> x, iterations, residual history.  Replaces
+ * solve_pcg / solve_fgmres with NativeCartesianMgPlan as preconditioner
+ * (include/hundun/v04_linear.hpp:1070-1088; src/solver_krylov.cpp:1299-1555,
+ * 1557-2650).  `solution` holds x0 on entry and x on success; on failure it
+ * is left unchanged.  `history` (may be NULL) receives the recursive
+ * residual norm after every iteration, up to `history_capacity` values. */
+HFPS_API int hfps_solve(hfps_solver* solver, const double* rhs, double* solution,
+               int memory, const hfps_control* control, hfps_result* result,
+               double* history, uint32_t history_capacity);
+
+/* y = A x with the IBM-decorated operator (LinearOperator::apply,
+ * include/hundun/v04_linear.hpp:396-405; src/solver_pressure.cpp:969-991). */
+HFPS_API int hfps_apply_operator(hfps_solver* solver, const double* x, double* y,
+                        int memory);
+
+/* z = M r, one MG preconditioner application (LinearPreconditioner::apply,
+ * include/hundun/v04_linear.hpp:418-420; src/solver_mg.cpp:4814-5122). */
+HFPS_API int hfps_apply_preconditioner(hfps_solver* solver, const double* r, double* z,
+                              int memory, int precision);
+
+/* Adjoint of a converged solve: solves A^T lambda = dL/dp (A is symmetric,
+ * so the forward solver is reused) and forms dL/dc_f = -(lambda_i -
+ * lambda_j)(p_i - p_j) per interior face (-lambda_i p_i on a Dirichlet
+ * boundary face; 0 on Neumann and IBM-removed faces), dL/drhs = lambda.
+ * Any of lambda/grad_* may be NULL.  No reference counterpart: the reference
+ * has no adjoint path. */
+HFPS_API int hfps_adjoint(hfps_solver* solver, const double* solution,
+                 const double* dl_dp, double* lambda, double* grad_face_x,
+                 double* grad_face_y, double* grad_face_z, int memory,
+                 const hfps_control* control, hfps_result* result);
+
+/* Level shapes: writes [nx, ny, nz, line_axis_mask] per level (up to
+ * capacity levels) and returns the level count (NativeCartesianMgPlan::level,
+ * include/hundun/v04_linear.hpp:968-969). */
+HFPS_API int hfps_levels(hfps_solver* solver, int* shapes, int capacity);
+
+/* Copies one level's masked/aggregated coefficients to host arrays (any may
+ * be NULL); `volume` receives the fluid volume per cell. */
+HFPS_API int hfps_level_coefficients(hfps_solver* solver, int level, double* diagonal,
+                            double* face_x, double* face_y, double* face_z,
+                            double* volume);
+
+/* Kernel classes timed by hfps_profile_kernel. */
+typedef enum hfps_kernel {
+  HFPS_KERNEL_OPERATOR = 0,        /* level-0 FP64 stencil y = A x with x.y */
+  HFPS_KERNEL_SMOOTH_FP64 = 1,     /* one level-0 smoother pass, FP64 */
+  HFPS_KERNEL_SMOOTH_FP32 = 2,     /* one level-0 smoother pass, FP32 */
+  HFPS_KERNEL_RESTRICT_FP64 = 3,   /* fused level-0 defect + restriction */
+  HFPS_KERNEL_PROLONG_FP64 = 4,    /* level-1 -> level-0 prolongation */
+  HFPS_KERNEL_PCG_UPDATE = 5,      /* x += a p, r -= a Ap, |r|^2 */
+  HFPS_KERNEL_MG_FP64 = 6,         /* one whole FP64 MG application */
+  HFPS_KERNEL_MG_MIXED = 7         /* one whole FP32 MG application */
+} hfps_kernel;
+
+/* Launches one kernel class `repetitions` times on the solver's stream
+ * between CUDA events, on the solver's current data, and reports the mean
+ * device time per launch and the algorithmic HBM bytes one launch must move
+ * (each operand read or written once).  Scratch vectors are overwritten; the
+ * coefficients are not.  No reference counterpart: the reference's
+ * MgApplyProfile (include/hundun/v04_linear.hpp:191-230) times host phases. */
+HFPS_API int hfps_profile_kernel(hfps_solver* solver, int kernel,
+                                 int repetitions, double* milliseconds,
+                                 double* bytes);
+
+/* Sticky error text of the last failing call on this handle. */
+HFPS_API const char* hfps_last_error(hfps_solver* solver);
+
+HFPS_API int hfps_destroy(hfps_solver* solver);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HF_PRESSURE_SOLVER_H */

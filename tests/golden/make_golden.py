@@ -1,0 +1,92 @@
+"""Generates the golden fixtures in tests/golden/ from the compiled reference.
+
+Run in a tree where the reference sources are present:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+For each small case the script builds the seeded system with
+hfps.workloads, then records what the reference's own code returns for it
+(oracle/_ref: NativeCartesianMgPlan::apply, the IBM-decorated operator and
+solve_pcg with the MG plan): the MG correction of a seeded vector, the
+operator action, and the solution/iteration count at rtol 1e-13.  A checksum
+of the inputs pins the generator, so a changed generator fails the tests
+instead of silently comparing different systems.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "hundun-flow_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from hfps import workloads  # noqa: E402
+import ref_oracle  # noqa: E402
+
+CASES = {
+    # name: (builder kwargs, policy kwargs)
+    "sphere_24x20x16_rbV22": (dict(config="sphere64", n=(24, 20, 16)), dict()),
+    "sphere_24x20x16_prodF": (dict(config="sphere64", n=(24, 20, 16)),
+                              dict(smoother=1, cycle=1, pre=1, post=2, diagonal_shortcut=0.1)),
+    "sphere_33x17x9_rbF22": (dict(config="sphere64", n=(33, 17, 9)), dict(cycle=1)),
+    "wrinkled_16x40x12_lineF": (dict(config="wrinkled256", n=(16, 40, 12), stretch_y=1.1),
+                                dict(smoother=1, cycle=1, pre=1, post=2)),
+}
+
+
+def system_for(spec):
+    spec = dict(spec)
+    name = spec.pop("config")
+    return workloads.make(name, **spec)
+
+
+def input_digest(system) -> str:
+    h = hashlib.sha256()
+    for a in (system.diagonal, system.face_x, system.face_y, system.face_z, system.rhs,
+              *system.faces):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    if system.active is not None:
+        h.update(np.ascontiguousarray(system.active, dtype=np.uint8).tobytes())
+    return h.hexdigest()
+
+
+def probe_vector(system, seed=99):
+    return np.ascontiguousarray(
+        workloads.normals(seed, system.cells).reshape(system.rhs.shape))
+
+
+def main():
+    if not ref_oracle.available():
+        raise SystemExit("build oracle/_ref first: make -C oracle ref")
+    index = {}
+    for name, (spec, pol) in CASES.items():
+        system = system_for(spec)
+        policy = ref_oracle.MgPolicy(**pol)
+        ref = ref_oracle.RefSession(system, policy, algorithm="pcg")
+        v = probe_vector(system)
+        mg = ref.apply_mg(v)
+        op = ref.apply_operator(v)
+        x, info = ref.solve(system.rhs, rtol=1e-13, maxit=400)
+        x10, info10 = ref.solve(system.rhs, rtol=1e-10, maxit=400)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), mg=mg, op=op, x=x, x10=x10)
+        index[name] = {
+            "spec": spec, "policy": pol, "digest": input_digest(system),
+            "levels": ref.levels(),
+            "iterations_1e13": info["iterations"], "iterations_1e10": info10["iterations"],
+            "final_true_residual_1e13": info["final_true_residual"],
+            "rhs_norm": info["rhs_norm"],
+        }
+        ref.close()
+        print(name, index[name]["iterations_1e13"], index[name]["iterations_1e10"])
+    with open(os.path.join(HERE, "index.json"), "w") as f:
+        json.dump(index, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,180 @@
+"""CPU tests of the oracle: the C restatement against the reference itself.
+
+The C restatement (oracle/hfps_oracle.c) is pinned three ways:
+* against golden fixtures recorded from the compiled reference sources
+  (tests/golden/make_golden.py): operator action, MG correction and the
+  solve_pcg solution must match bit for bit;
+* against the compiled reference live, when oracle/_ref is present;
+* against the reference's own known-answer and property tests, ported:
+  Chebyshev degrees 1-4 (tests/unit/solver_mg_chebyshev_test.cpp:797-841),
+  IBM operator equivalence (tests/unit/solver_ibm_pressure_operator_test.cpp:
+  131-233), monotone MG contraction (tests/numerical/
+  solver_mg_convergence_test.cpp:630-800) and PCG against an independent
+  direct solve (tests/mpi/solver_krylov_mpi_test.cpp:1141-1193).
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import golden_cases
+from hfps import workloads
+
+pytestmark = pytest.mark.usefixtures("oracle_built")
+
+
+def _oracle(system, policy, unit_linear=True, line_order=0):
+    import c_oracle
+    return c_oracle.OracleSession(system, policy, unit_linear=unit_linear, line_order=line_order)
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.index()))
+def test_generator_matches_recorded_inputs(name):
+    s = golden_cases.system(name)
+    assert golden_cases.digest(s) == golden_cases.index()[name]["digest"]
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.index()))
+def test_restatement_reproduces_reference_golden(name):
+    s = golden_cases.system(name)
+    g = golden_cases.arrays(name)
+    meta = golden_cases.index()[name]
+    o = _oracle(s, golden_cases.policy(name))
+    assert [list(l) for l in o.levels()] == meta["levels"]
+    v = golden_cases.probe(s)
+    assert np.array_equal(o.apply_operator(v), g["op"])
+    assert np.array_equal(o.apply_mg(v), g["mg"])
+    x, info = o.solve(s.rhs, rtol=1e-13, maxit=400)
+    assert info["termination"] == "converged"
+    assert info["iterations"] == meta["iterations_1e13"]
+    assert np.array_equal(x, g["x"])
+
+
+def test_restatement_matches_live_reference():
+    import ref_oracle
+    if not ref_oracle.available():
+        pytest.skip("compiled reference not built (make -C oracle ref)")
+    s = workloads.make("sphere64", n=(20, 13, 11), spheres=((0.4, 0.45, 0.5, 0.2),), seed=5)
+    for pol in (ref_oracle.MgPolicy(), ref_oracle.MgPolicy.production(),
+                ref_oracle.MgPolicy(cycle=1, pre=3, post=1, coarse_sweeps=7)):
+        r = ref_oracle.RefSession(s, pol, algorithm="pcg")
+        o = _oracle(s, pol)
+        v = golden_cases.probe(s)
+        assert np.array_equal(r.apply_mg(v), o.apply_mg(v))
+        x1, i1 = r.solve(s.rhs, rtol=1e-11)
+        x2, i2 = o.solve(s.rhs, rtol=1e-11)
+        assert i1["iterations"] == i2["iterations"]
+        assert np.array_equal(x1, x2)
+
+
+def _uniform_system(n, diag, face, boundary=(0, 0, 0, 0, 0, 0), active=None, rhs=None):
+    nx, ny, nz = n
+    faces = tuple(workloads.uniform_faces(m) for m in n)
+    fx = np.full((nz, ny, nx + 1), face)
+    fy = np.full((nz, ny + 1, nx), face)
+    fz = np.full((nz + 1, ny, nx), face)
+    d = np.full((nz, ny, nx), diag)
+    if rhs is None:
+        rhs = np.zeros((nz, ny, nx))
+    return workloads.PressureSystem("uniform", (nx, ny, nz), faces, tuple(boundary),
+                                    np.ones((nz, ny, nx)), d, fx, fy, fz, active, rhs)
+
+
+def _scalar_chebyshev(rhs, diagonal, eigenvalue, stages, fraction):
+    beta = 2.0
+    alpha = fraction * beta
+    theta = (beta + alpha) * 0.5
+    delta = (beta - alpha) * 0.5
+    sigma = theta / delta
+    x = 0.0
+    d = 0.0
+    prev = 1.0 / sigma
+    for s in range(stages):
+        defect = rhs - eigenvalue * x
+        if s == 0:
+            d = defect / (theta * diagonal)
+        else:
+            rho = 1.0 / (2.0 * sigma - prev)
+            d = rho * prev * d + (2.0 * rho / delta) * defect / diagonal
+            prev = rho
+        x += d
+    return x
+
+
+@pytest.mark.parametrize("degree", [1, 2, 3, 4])
+def test_chebyshev_known_answer(degree):
+    """Degree-d Chebyshev pre/post smoothing on A = 2I with alternating rhs
+    has a closed form: the coarse correction of the alternating field is 0
+    (solver_mg_chebyshev_test.cpp:797-841)."""
+    import ref_oracle
+    n = (8, 8, 8)
+    i, j, k = np.meshgrid(np.arange(8), np.arange(8), np.arange(8), indexing="ij")
+    sign = np.where(((i + j + k) & 1) == 0, 1.0, -1.0).transpose(2, 1, 0)
+    s = _uniform_system(n, 2.0, 0.0, rhs=np.ascontiguousarray(sign))
+    pol = ref_oracle.MgPolicy(smoother=1, pre=degree, post=degree)
+    o = _oracle(s, pol)
+    z = o.apply_mg(s.rhs)
+    pre = _scalar_chebyshev(1.0, 2.0, 2.0, degree, 0.3)
+    post = _scalar_chebyshev(1.0 - 2.0 * pre, 2.0, 2.0, degree, 0.3)
+    assert np.max(np.abs(z - sign * (pre + post))) < 2e-12
+
+
+def test_ibm_decoration_equals_masked_operator():
+    """Decorated regular operator == compact operator with removed faces
+    (solver_ibm_pressure_operator_test.cpp:131-233, tolerance 2e-12)."""
+    s = workloads.make("sphere64", n=(18, 16, 14), spheres=((0.45, 0.5, 0.5, 0.25),))
+    o = _oracle(s, None)
+    v = golden_cases.probe(s)
+    decorated = o.apply_operator(v)
+    masked = o.apply_level(0, v)
+    scale = np.max(np.abs(decorated))
+    assert np.max(np.abs(decorated - masked)) <= 2e-12 * scale
+    solid = s.active == 0
+    assert np.array_equal(decorated[solid], v[solid])
+
+
+def test_mg_cycles_contract_monotonically():
+    """Residual-minimising MG as a stationary iteration reduces the true
+    residual monotonically (solver_mg_convergence_test.cpp:630-800)."""
+    import ref_oracle
+    s = workloads.make("wrinkled256", n=(16, 12, 8), stretch_y=None, seed=3)
+    o = _oracle(s, ref_oracle.MgPolicy(), unit_linear=False)
+    x = np.zeros_like(s.rhs)
+    r = s.rhs - o.apply_operator(x)
+    norms = [np.linalg.norm(r)]
+    for _ in range(10):
+        x = x + o.apply_mg(r)
+        r = s.rhs - o.apply_operator(x)
+        norms.append(np.linalg.norm(r))
+    assert all(b <= a * (1 + 1e-12) for a, b in zip(norms, norms[1:]))
+    assert norms[-1] <= 0.5 * norms[0]
+
+
+def test_pcg_matches_direct_solve():
+    """solve_pcg with MG against an independent sparse direct solve
+    (solver_krylov_mpi_test.cpp:1141-1193: error < 1e-8)."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    s = workloads.make("sphere64", n=(12, 10, 9), spheres=((0.5, 0.5, 0.5, 0.2),), seed=2)
+    o = _oracle(s, None)
+    n = s.cells
+    cols = []
+    for c in range(n):
+        e = np.zeros(n)
+        e[c] = 1.0
+        cols.append(sp.csc_matrix(o.apply_operator(e.reshape(s.rhs.shape)).reshape(-1, 1)))
+    A = sp.hstack(cols).tocsc()
+    exact = spla.spsolve(A, s.rhs.reshape(-1)).reshape(s.rhs.shape)
+    x, info = o.solve(s.rhs, rtol=1e-13)
+    assert info["termination"] == "converged"
+    assert np.linalg.norm(x - exact) / np.linalg.norm(exact) < 1e-8
+
+
+def test_zero_rhs_and_converged_guess():
+    s = workloads.make("sphere64", n=(8, 8, 8))
+    o = _oracle(s, None)
+    x, info = o.solve(np.zeros_like(s.rhs))
+    assert info["termination"] == "zero_rhs" and not np.any(x)
+    x1, _ = o.solve(s.rhs, rtol=1e-12)
+    x2, info2 = o.solve(s.rhs, x0=x1, rtol=1e-10)
+    assert info2["iterations"] == 0 and info2["termination"] == "converged"
