@@ -288,9 +288,11 @@ def run_b200(args, world, rank, local):
     e2e_seconds = max_over_ranks(world, time.perf_counter() - t0)
     e2e_value = world * args.steps / e2e_seconds
 
-    # Dominant kernel: the level-0 line-relaxation colour pass (largest share
-    # of device time in the launch list).  Timed with CUDA events on the
-    # solver's stream; algorithmic bytes = 28 B per level-0 cell per pass.
+    # Dominant kernel: the level-0 zebra line-relaxation colour pass (largest
+    # share of device time in the launch list).  Timed with CUDA events on
+    # the solver's stream; algorithmic bytes = 28 B per level-0 cell per pass
+    # (each operand of a full sweep x, b, D, fx, fy, fz and the x write read
+    # or written once over the two colour passes).
     kernels = {}
     for name in ("smooth_fp64", "operator", "restrict_fp64", "prolong_fp64", "pcg_update",
                  "smooth_fp32", "mg_fp64", "mg_mixed"):
@@ -305,7 +307,8 @@ def run_b200(args, world, rank, local):
     else:
         peak, peak_note = 6650.0, "fallback"
     dom = kernels["smooth_fp64"]
-    roofline = {"bound": "hbm", "kernel": "k_line_color<double> level 0 (one zebra colour)",
+    roofline = {"bound": "hbm",
+                "kernel": "k_line_segment_color<double,y,8> level 0 (one zebra colour)",
                 "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": dom["gbs"] / peak, "peak_source": peak_note,
                 "traffic": None, "bytes_per_launch": dom["bytes"], "ms_per_launch": dom["ms"]}

@@ -49,9 +49,8 @@ __device__ __forceinline__ int face_y_index(const Level<T>& L, int c, int k) {
 
 // A x at one cell, in the reference's accumulation order.
 template <class T>
-__device__ __forceinline__ T row_value(const Level<T>& L,
-                                       const T* __restrict__ x, int i, int j,
-                                       int k, int c) {
+__device__ __forceinline__ T row_value(const Level<T>& L, const T* x, int i,
+                                       int j, int k, int c) {
   const int plane = L.nx * L.ny;
   const T xc = x[c];
   const T xm = i > 0 ? x[c - 1] : ((L.neumann & 1u) ? xc : T(0));
@@ -74,11 +73,12 @@ __device__ __forceinline__ T row_value(const Level<T>& L,
 
 // Neighbour along `axis` in direction `dir` for the line smoother's
 // transverse and end terms (level_neighbor, src/solver_mg.cpp:2222-2262).
+// x may live in shared memory that other threads update between barriers
+// (coarsest-level kernels), so it is not __restrict__-qualified.
 template <class T>
-__device__ __forceinline__ T line_neighbour(const Level<T>& L,
-                                            const T* __restrict__ x, int i,
-                                            int j, int k, int c, int axis,
-                                            int dir) {
+__device__ __forceinline__ T line_neighbour(const Level<T>& L, const T* x,
+                                            int i, int j, int k, int c,
+                                            int axis, int dir) {
   if (axis == 0) {
     if (dir < 0) return i > 0 ? x[c - 1] : ((L.neumann & 1u) ? x[c] : T(0));
     return i + 1 < L.nx ? x[c + 1] : ((L.neumann & 2u) ? x[c] : T(0));
@@ -95,9 +95,8 @@ __device__ __forceinline__ T line_neighbour(const Level<T>& L,
 // Row s of the line system through cell (fa, fb) along `axis`: the same
 // a, b, c, d the Thomas solve forms (src/solver_mg.cpp:3440-3478).
 template <class T>
-__device__ __forceinline__ void line_row(const Level<T>& L,
-                                         const T* __restrict__ x,
-                                         const T* __restrict__ rhs, int axis,
+__device__ __forceinline__ void line_row(const Level<T>& L, const T* x,
+                                         const T* rhs, int axis,
                                          int fa, int fb, int s, int& c, T& a,
                                          T& bb, T& cc, T& d) {
   const int extent = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);

@@ -178,10 +178,8 @@ __global__ void k_chebyshev_stage(Level<T> L, const T* __restrict__ x,
 
 // Thomas solve of one line (solve_one, src/solver_mg.cpp:3388-3493).
 template <class T>
-__device__ void line_thomas(const Level<T>& L, T* __restrict__ x,
-                            const T* __restrict__ b, T* __restrict__ work,
-                            T* __restrict__ dprime, int axis, int fa,
-                            int fb) {
+__device__ void line_thomas(const Level<T>& L, T* x, const T* b, T* work,
+                            T* dprime, int axis, int fa, int fb) {
   const int extent = axis == 0 ? L.nx : (axis == 1 ? L.ny : L.nz);
   const int plane = L.nx * L.ny;
   const int stride = axis == 0 ? 1 : (axis == 1 ? L.nx : plane);
@@ -366,10 +364,9 @@ __global__ void k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C,
 // branch, src/solver_mg.cpp:4210-4227).  The state is widened to TC (FP64
 // in the mixed-precision hierarchy) for the duration of the solve.
 template <class T, class TC>
-__global__ void k_coarse_solve(Level<TC> L, T* __restrict__ x,
-                               const T* __restrict__ b, TC* __restrict__ xs,
-                               TC* __restrict__ bs, TC* __restrict__ work,
-                               TC* __restrict__ dprime, int sweeps,
+// x / xs are updated by every thread between barriers: no __restrict__.
+__global__ void k_coarse_solve(Level<TC> L, T* x, const T* b, TC* xs, TC* bs,
+                               TC* work, TC* dprime, int sweeps,
                                int line_axis) {
   const int n = L.nx * L.ny * L.nz;
   TC* xw = xs;

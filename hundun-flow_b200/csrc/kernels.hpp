@@ -70,17 +70,19 @@ template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int coarsen_mask);
 // ---- zebra line relaxation (kernels_line.cu) --------------------------------
-// Line-colour passes with more lines than this run one Thomas recurrence per
-// thread; fewer lines run PCR with one CTA row per line.
-constexpr long long kLinePcrThreshold = 4096;
-enum LineKind : int { kLineNone = 0, kLineThomas = 1, kLinePcr = 2 };
+// Line-colour passes with more lines than this run the partition method
+// (one warp per line segment, lanes across lines); fewer lines run PCR with
+// one CTA row per line.
+constexpr long long kLinePcrThreshold = 1024;
+enum LineKind : int { kLineNone = 0, kLineSegment = 1, kLinePcr = 2 };
 int line_kind(int nx, int ny, int nz, int axis);
-// Values of the factor block of one level and line axis: Thomas c' and
-// denominators (2 per cell) or PCR multipliers and final diagonals.
+// Values of the factor block of one level and line axis: segment-local
+// Thomas factors and spikes (4 per cell) plus the per-line interface
+// inverse, or PCR multipliers and final diagonals.
 size_t line_factor_values(int nx, int ny, int nz, int axis);
 template <class T>
 void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac);
-// One zebra colour; `scratch` holds the Thomas d' values (cells).
+// One zebra colour of line relaxation along `axis`.
 template <class T>
 void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
                       const T* fac, T* scratch, int axis, int color);
