@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBRARY = os.path.join(HERE, "libhfps.so")
-SOURCES = ["kernels.cu", "kernels_line.cu", "solver.cu", "capi.cu"]
+SOURCES = ["kernels.cu", "kernels_line.cu", "solver.cu", "capi.cu", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",

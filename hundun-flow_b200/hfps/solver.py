@@ -110,13 +110,21 @@ class Result(ctypes.Structure):
         return d
 
 
+class OperatorView(ctypes.Structure):
+    """hfps_operator_view: device coefficient arrays of the finest level."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("boundary", ctypes.c_int * 6),
+                ("diagonal", ctypes.c_void_p), ("face_x", ctypes.c_void_p),
+                ("face_y", ctypes.c_void_p), ("face_z", ctypes.c_void_p)]
+
+
 _LIB = None
 
 EXPORTS = ["hfps_default_policy", "hfps_production_policy", "hfps_default_control",
            "hfps_create", "hfps_set_coefficients", "hfps_set_beta", "hfps_solve",
            "hfps_apply_operator", "hfps_apply_preconditioner", "hfps_adjoint",
            "hfps_levels", "hfps_level_coefficients", "hfps_profile_kernel",
-           "hfps_last_error", "hfps_destroy"]
+           "hfps_operator_dot_noalloc", "hfps_last_error", "hfps_destroy"]
 
 KERNELS = {"operator": 0, "smooth_fp64": 1, "smooth_fp32": 2, "restrict_fp64": 3,
            "prolong_fp64": 4, "pcg_update": 5, "mg_fp64": 6, "mg_mixed": 7}
@@ -148,6 +156,7 @@ def _lib():
         lib.hfps_profile_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]
+        lib.hfps_operator_dot_noalloc.argtypes = [ctypes.POINTER(OperatorView), vp, vp, vp, vp]
         lib.hfps_last_error.argtypes = [vp]
         lib.hfps_last_error.restype = ctypes.c_char_p
         lib.hfps_destroy.argtypes = [vp]

@@ -236,6 +236,49 @@ HFPS_API int hfps_profile_kernel(hfps_solver* solver, int kernel,
                                  int repetitions, double* milliseconds,
                                  double* bytes);
 
+/* ---- Allocation-free operator apply ------------------------------------
+ * No counterpart in the reference.  Every other entry point works through a
+ * solver handle whose workspaces were allocated by hfps_create.  Some callers
+ * cannot allocate device memory at the point where they need A x: a step
+ * running inside a fixed memory pool or a caching allocator that forbids new
+ * device allocations mid-step, or code that must keep a fixed footprint.
+ * This entry point serves them.  It works on device arrays the caller
+ * already owns, never allocates device or pinned memory, and keeps its
+ * reduction scratch in a fixed array inside the library.
+ *
+ * It computes y = A x and, when x_dot_y is not NULL, x . (A x).  The
+ * coefficients are the IBM-masked finest-level ones, laid out as
+ * hfps_level_coefficients(solver, 0, ...) returns them: solid cells have an
+ * identity row, removed faces are 0.  All arrays are device memory on the
+ * current CUDA device; `stream` is a cudaStream_t (NULL: the default stream).
+ * The call is asynchronous: y and *x_dot_y are ready when the stream is.
+ *
+ * The first call on each device does a one-time set-up: it looks up the
+ * address of the library's scratch array on that device.  Make that first
+ * call before any stream capture begins.  The scratch array is shared by
+ * every call on a device, so calls that overlap in time (two streams, two
+ * host threads) race and give wrong results: serialise them.
+ *
+ * Returns HFPS_OK, HFPS_INVALID_CASE when an extent is below 1 or the grid
+ * has more than HFPS_NOALLOC_MAX_CELLS cells, or HFPS_INVALID_PLAN for a
+ * periodic or unknown boundary kind, a NULL, misaligned or non-device
+ * pointer, y overlapping x, or a CUDA runtime error. */
+#define HFPS_NOALLOC_MAX_CELLS (1LL << 30)   /* 32-bit face indexing */
+#define HFPS_NOALLOC_MAX_BLOCKS 1184         /* reduction partials kept */
+
+typedef struct hfps_operator_view {
+  int nx, ny, nz;
+  int boundary[6];            /* hfps_boundary per face, x_min..z_max */
+  const double* diagonal;     /* nx*ny*nz */
+  const double* face_x;       /* (nx+1)*ny*nz */
+  const double* face_y;       /* nx*(ny+1)*nz */
+  const double* face_z;       /* nx*ny*(nz+1) */
+} hfps_operator_view;
+
+HFPS_API int hfps_operator_dot_noalloc(const hfps_operator_view* op,
+                                       const double* x, double* y,
+                                       double* x_dot_y, void* stream);
+
 /* Sticky error text of the last failing call on this handle. */
 HFPS_API const char* hfps_last_error(hfps_solver* solver);
 

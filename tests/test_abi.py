@@ -63,3 +63,18 @@ def test_missing_gpu_fails_loudly(cuda_library):
     faces = [np.linspace(0, 1, 9)] * 3
     with pytest.raises(SolverError):
         PressureSolver((8, 8, 8), faces, (0,) * 6)
+
+
+def test_noalloc_rejects_oversize_grids_before_any_device_call(cuda_library):
+    """Grids beyond HFPS_NOALLOC_MAX_CELLS (or with an empty extent) are
+    refused from the sizes alone, before the entry point touches the GPU."""
+    from hfps import solver as binding
+    lib = binding._lib()
+    v = binding.OperatorView()
+    v.nx = v.ny = v.nz = 1100                      # 1.33e9 cells > 2**30
+    assert lib.hfps_operator_dot_noalloc(ctypes.byref(v), None, None, None, None) == 1
+    v.nx = 0
+    assert lib.hfps_operator_dot_noalloc(ctypes.byref(v), None, None, None, None) == 1
+    assert lib.hfps_operator_dot_noalloc(None, None, None, None, None) == 2
+    header = open(HEADER).read()
+    assert "#define HFPS_NOALLOC_MAX_CELLS (1LL << 30)" in header
