@@ -308,7 +308,7 @@ def run_b200(args, world, rank, local):
         peak, peak_note = 6650.0, "fallback"
     dom = kernels["smooth_fp64"]
     roofline = {"bound": "hbm",
-                "kernel": "k_line_segment_color<double,y,8> level 0 (one zebra colour)",
+                "kernel": "k_line_scan_color<double,y,8> level 0 (one zebra colour)",
                 "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": dom["gbs"] / peak, "peak_source": peak_note,
                 "traffic": None, "bytes_per_launch": dom["bytes"], "ms_per_launch": dom["ms"]}
@@ -330,7 +330,7 @@ def run_b200(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": 1000.0 * seconds / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded SplitMix64/Box-Muller face-flux divergence)",
-            "config": {"workload": "wrinkled256 warm-start pressure solve (configs[1])",
+            "config": {"workload": "wrinkled256 warm-start pressure solve (256^3 stretched, 20-step sequence)",
                        "shape": list(system.shape), "stretch_y": 1.02,
                        "algorithm": "PCG (solve_pcg control flow) + MG production policy, unit_linear",
                        "rtol": RTOL, "true_residual_interval": TRUE_RESIDUAL_INTERVAL,

@@ -70,15 +70,16 @@ template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int coarsen_mask);
 // ---- zebra line relaxation (kernels_line.cu) --------------------------------
-// Line-colour passes with more lines than this run the partition method
-// (one warp per line segment, lanes across lines); fewer lines run PCR with
-// one CTA row per line.
+// Line-colour passes with more lines than this run the chunked-scan solve
+// (lanes across lines, warps along chunks of one line); fewer lines run PCR
+// with one CTA row per line.  Lines longer than 2048 cells are not
+// supported (kLineNone).
 constexpr long long kLinePcrThreshold = 1024;
-enum LineKind : int { kLineNone = 0, kLineSegment = 1, kLinePcr = 2 };
+enum LineKind : int { kLineNone = 0, kLineScan = 1, kLinePcr = 2 };
 int line_kind(int nx, int ny, int nz, int axis);
-// Values of the factor block of one level and line axis: segment-local
-// Thomas factors and spikes (4 per cell) plus the per-line interface
-// inverse, or PCR multipliers and final diagonals.
+// Values of the factor block of one level and line axis: the Thomas
+// reciprocal, lower multiplier and upper multiplier (3 per cell), or PCR
+// multipliers and final diagonals.
 size_t line_factor_values(int nx, int ny, int nz, int axis);
 template <class T>
 void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac);

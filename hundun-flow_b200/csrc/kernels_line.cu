@@ -7,12 +7,11 @@
 // them are solved at once.  The line matrices depend only on the level
 // coefficients, so every factorisation is computed once per coefficient
 // update and each sweep does only right-hand-side work:
-//   * many lines per colour: the partition method.  Each line is cut into
-//     S segments; a warp solves one segment of 32 lines (lanes run across
-//     lines, so loads coalesce along x), the S segment solutions are
-//     coupled through a 2S x 2S interface system whose inverse is stored
-//     per line, and the segment-local Thomas factors and the two spike
-//     vectors of every segment are stored per cell;
+//   * many lines per colour: a chunked scan over precomputed Thomas
+//     factors.  Lanes run across lines (loads coalesce along x), each
+//     thread owns a chunk of up to 16 rows of its line, and the chunks of a
+//     line combine the affine maps of the forward and backward recurrences
+//     through shared memory;
 //   * few lines per colour (coarse levels): one CTA row per line runs
 //     parallel cyclic reduction with precomputed elimination factors held
 //     in registers;
@@ -25,9 +24,6 @@
 namespace hfps {
 namespace {
 
-constexpr int kLanes = 32;
-constexpr int kMaxSegments = 8;
-constexpr int kChunk = 4;
 
 __host__ __device__ __forceinline__ int line_extent(int axis, int nx, int ny,
                                                     int nz) {
@@ -109,63 +105,175 @@ __device__ __forceinline__ T line_rhs(const Level<T>& L, const T* x,
   return d;
 }
 
+// Right-hand side of the rows of one line with everything that is constant
+// along the line hoisted: the transverse neighbours' offsets (0 where the
+// neighbour is outside the level, read as 0 for Dirichlet and as the cell
+// itself for Neumann), the face arrays with their index at row 0 and stride
+// per row, and the line-end boundary faces.  Every load of a row is
+// unconditional, so a thread can keep many rows' loads in flight.  The
+// arithmetic and its order are line_rhs's.  Transverse neighbours belong to
+// the other colour, which a colour pass never writes, so they are read
+// through the read-only path.
+template <class T, int AXIS>
+struct LineRhs {
+  static constexpr int kA0 = AXIS == 0 ? 1 : 0;  // first transverse axis
+  static constexpr int kA1 = AXIS == 2 ? 1 : 2;  // second transverse axis
+  const T* face[2];
+  int fbase[2], fstride[2], fhigh[2];
+  int off[4];
+  bool keep[4];
+  T end_low, end_high;   // line-end boundary faces (rows 0 and extent-1)
+  bool lkeep_low, lkeep_high;
+
+  __device__ static void axis_faces(const Level<T>& L, int axis, int i, int j,
+                                    int k, int line_axis, const T*& f,
+                                    int& b, int& st, int& hi) {
+    // Face index of cell (i, j, k) on `axis`, its step per row along
+    // line_axis, and the offset of the cell's high face.
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    if (axis == 0) {
+      f = L.fx;
+      b = i + (nx + 1) * (j + ny * k);
+      st = line_axis == 0 ? 1 : (line_axis == 1 ? nx + 1 : (nx + 1) * ny);
+      hi = 1;
+    } else if (axis == 1) {
+      f = L.fy;
+      b = i + nx * (j + (ny + 1) * k);
+      st = line_axis == 0 ? 1 : (line_axis == 1 ? nx : nx * (ny + 1));
+      hi = nx;
+    } else {
+      f = L.fz;
+      b = i + nx * (j + ny * k);
+      st = line_axis == 0 ? 1 : (line_axis == 1 ? nx : nx * ny);
+      hi = nx * ny;
+    }
+    (void)nz;
+  }
+
+  __device__ LineRhs(const Level<T>& L, int fa, int fb) {
+    int i0, j0, k0;
+    line_cell(AXIS, fa, fb, 0, i0, j0, k0);
+    const int idx[3] = {i0, j0, k0};
+    const int ext[3] = {L.nx, L.ny, L.nz};
+    const int step[3] = {1, L.nx, L.nx * L.ny};
+    const int axes[2] = {kA0, kA1};
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+      const int a = axes[n];
+      axis_faces(L, a, i0, j0, k0, AXIS, face[n], fbase[n], fstride[n], fhigh[n]);
+      const bool low_in = idx[a] > 0, high_in = idx[a] + 1 < ext[a];
+      off[2 * n] = low_in ? -step[a] : 0;
+      off[2 * n + 1] = high_in ? step[a] : 0;
+      keep[2 * n] = low_in || ((L.neumann >> (2 * a)) & 1u);
+      keep[2 * n + 1] = high_in || ((L.neumann >> (2 * a + 1)) & 1u);
+    }
+    const T* lface;
+    int lbase, lstride, lhigh;
+    axis_faces(L, AXIS, i0, j0, k0, AXIS, lface, lbase, lstride, lhigh);
+    end_low = __ldg(lface + lbase);
+    end_high = __ldg(lface + lbase + (ext[AXIS] - 1) * lstride + lhigh);
+    lkeep_low = (L.neumann >> (2 * AXIS)) & 1u;
+    lkeep_high = (L.neumann >> (2 * AXIS + 1)) & 1u;
+  }
+
+  __device__ __forceinline__ T row(const T* x, const T* __restrict__ rhs, int c,
+                                   int s, int extent) const {
+    T d = __ldg(rhs + c);
+#pragma unroll
+    for (int n = 0; n < 2; ++n) {
+      const int f = fbase[n] + s * fstride[n];
+      const T lo = __ldg(x + c + off[2 * n]);
+      const T hi = __ldg(x + c + off[2 * n + 1]);
+      d += __ldg(face[n] + f) * (keep[2 * n] ? lo : T(0));
+      d += __ldg(face[n] + f + fhigh[n]) * (keep[2 * n + 1] ? hi : T(0));
+    }
+    const T self = x[c];
+    const T dl = d + end_low * (lkeep_low ? self : T(0));
+    d = s == 0 ? dl : d;
+    const T dh = d + end_high * (lkeep_high ? self : T(0));
+    return s + 1 == extent ? dh : d;
+  }
+};
+
 // ---------------------------------------------------------------------------
-// Partition method.
+// Chunked-scan line solve.
 //
-// Segment q holds rows [r0, r1].  With its couplings to x_{r0-1} and
-// x_{r1+1} moved to the right-hand side, T_q x = d - a_{r0} x_{r0-1} e_0 -
-// c_{r1} x_{r1+1} e_m, so x = y - v x_{r0-1} - w x_{r1+1} with y = T_q^-1 d
-// and the spikes v = T_q^-1 a_{r0} e_0, w = T_q^-1 c_{r1} e_m.  The first
-// and last unknowns F_q, L_q of all segments solve a 2S x 2S system whose
-// inverse R is stored per line.
+// Each line's matrix is factorised once (full-line Thomas, in FP64): for row
+// s, den_s = b_s - a_s c'_{s-1}, and the sweep needs only
+//   inv_s = 1 / den_s,   l_s = a_s / den_s,   u_s = c'_s = c_s / den_s.
+// A sweep is then two first-order linear recurrences,
+//   forward   y_s = d_s inv_s - l_s y_{s-1},
+//   backward  x_s = y_s - u_s x_{s+1},
+// each an affine map per row.  A thread owns a chunk of up to
+// ScanConfig<T>::rows consecutive rows of one line: it composes its chunk's
+// maps, the chunks of a line combine their compositions through shared
+// memory, and every thread replays its chunk from the incoming value.  No spike vectors or interface
+// systems are stored, no division happens in a sweep, and the right-hand
+// side of a chunk (the costly part: rhs, transverse faces and neighbours)
+// stays in registers between the passes.
 //
-// Factor layout is colour-packed so that the 32 lanes of a warp (32 lines
-// of one colour, consecutive along the transverse index) read consecutive
-// addresses: array e of row s of colour line t sits at
-//   ((e * 2 + colour) * extent + s) * colour_lines + t,
-// e = 0 local denominator, 1 local c', 2 spike v, 3 spike w, 4 sub-diagonal
-// a; and R entry (r, c) of that line at
-//   ((r * 2S + c) * 2 + colour) * colour_lines + t.
+// Factor layout is colour-packed so that threads with consecutive line
+// indices of one colour read consecutive addresses: array e (0 inv, 1 l,
+// 2 u) of row s of colour line t sits at
+//   ((e * 2 + colour) * extent + s) * colour_lines + t.
 
-__host__ __device__ __forceinline__ void segment_rows(int extent, int S, int q,
-                                                      int& r0, int& r1) {
-  const int m = extent / S;
-  r0 = q * m;
-  r1 = q + 1 == S ? extent - 1 : r0 + m - 1;
-}
+// Rows per chunk (held in registers) and the block-size bound, per
+// precision: FP64 rows take twice the registers of FP32 rows.
+// Measured on B200 at 256^3 (level-0 y-line colour pass): FP64 16 rows in
+// blocks of <= 128 threads (8 lines x 16 chunks), FP32 8 rows in blocks of
+// <= 512 threads (16 lines x 32 chunks).
+#ifndef HFPS_SCAN_ROWS_F64
+#define HFPS_SCAN_ROWS_F64 16
+#endif
+#ifndef HFPS_SCAN_THREADS_F64
+#define HFPS_SCAN_THREADS_F64 128
+#endif
+#ifndef HFPS_SCAN_ROWS_F32
+#define HFPS_SCAN_ROWS_F32 8
+#endif
+#ifndef HFPS_SCAN_THREADS_F32
+#define HFPS_SCAN_THREADS_F32 512
+#endif
+template <class T>
+struct ScanConfig;
+template <>
+struct ScanConfig<double> {
+  static constexpr int rows = HFPS_SCAN_ROWS_F64;
+  static constexpr int threads = HFPS_SCAN_THREADS_F64;
+};
+template <>
+struct ScanConfig<float> {
+  static constexpr int rows = HFPS_SCAN_ROWS_F32;
+  static constexpr int threads = HFPS_SCAN_THREADS_F32;
+};
+// Longest line both precisions can solve: every chunk of a line lives in
+// one block.
+constexpr int kScanMaxExtent =
+    HFPS_SCAN_ROWS_F64 * HFPS_SCAN_THREADS_F64 < HFPS_SCAN_ROWS_F32 * HFPS_SCAN_THREADS_F32
+        ? HFPS_SCAN_ROWS_F64 * HFPS_SCAN_THREADS_F64
+        : HFPS_SCAN_ROWS_F32 * HFPS_SCAN_THREADS_F32;
+constexpr int kScanArrays = 3;
 
-__host__ __device__ __forceinline__ int segments_for(int extent) {
-  int S = kMaxSegments;
-  while (S > 1 && extent / S < 8) S >>= 1;
-  return S;
-}
-
-constexpr int kSegmentArrays = 5;
-
-struct SegmentLayout {
+struct ScanLayout {
   int extent;
   int colour_lines;
   __host__ __device__ size_t cell(int e, int colour, int s, int t) const {
     return ((static_cast<size_t>(e) * 2 + colour) * extent + s) * colour_lines + t;
   }
-  __host__ __device__ size_t cell_values() const {
-    return static_cast<size_t>(kSegmentArrays) * 2 * extent * colour_lines;
-  }
-  __host__ __device__ size_t rinv(int n2, int r, int c, int colour, int t) const {
-    return ((static_cast<size_t>(r) * n2 + c) * 2 + colour) * colour_lines + t;
+  __host__ __device__ size_t values() const {
+    return static_cast<size_t>(kScanArrays) * 2 * extent * colour_lines;
   }
 };
 
+// Thomas factors of every line, one thread per line, in FP64 whatever T is.
 template <class T>
-__global__ void k_segment_factors(Level<T> L, int axis, int S, T* __restrict__ fac) {
+__global__ void k_scan_factors(Level<T> L, int axis, T* __restrict__ fac) {
   const int a_extent = axis == 0 ? L.ny : L.nx;
   const int b_extent = axis == 2 ? L.ny : L.nz;
   const int lines = a_extent * b_extent;
   const int extent = line_extent(axis, L.nx, L.ny, L.nz);
   const int ha = (a_extent + 1) >> 1;
-  const SegmentLayout lay{extent, ha * b_extent};
-  T* rinv = fac + lay.cell_values();
-  const int n2 = 2 * S;
+  const ScanLayout lay{extent, ha * b_extent};
   for (int line = blockIdx.x * blockDim.x + threadIdx.x; line < lines;
        line += gridDim.x * blockDim.x) {
     const int fb = line / a_extent;
@@ -174,192 +282,109 @@ __global__ void k_segment_factors(Level<T> L, int axis, int S, T* __restrict__ f
     const int t = fb * ha + (fa >> 1);
     int base, stride;
     line_geometry(L, axis, fa, fb, base, stride);
-    for (int q = 0; q < S; ++q) {
-      int r0, r1;
-      segment_rows(extent, S, q, r0, r1);
-      // Local Thomas factorisation and the forward pass of spike v.
-      T prev_cl = T(0), prev_v = T(0), c_last = T(0);
-      for (int s = r0; s <= r1; ++s) {
-        const int c = base + s * stride;
-        int i, j, k;
-        line_cell(axis, fa, fb, s, i, j, k);
-        T lowf, highf;
-        line_faces(L, axis, c, j, k, lowf, highf);
-        const T a = s == 0 ? T(0) : -lowf;
-        const T cc = s + 1 == extent ? T(0) : -highf;
-        const T bb = L.diag[c];
-        const T d = s == r0 ? bb : bb - a * prev_cl;
-        const T w_local = cc / d;
-        const T vp = s == r0 ? a / d : (T(0) - a * prev_v) / d;
-        if (s == r1) c_last = cc;
-        fac[lay.cell(0, colour, s, t)] = d;
-        fac[lay.cell(1, colour, s, t)] = w_local;
-        fac[lay.cell(2, colour, s, t)] = vp;
-        fac[lay.cell(4, colour, s, t)] = a;
-        prev_cl = w_local;
-        prev_v = vp;
-      }
-      // Backward passes: v = v' - c' v_next; w' is zero but for the last row.
-      T next_v = T(0), next_w = T(0);
-      for (int s = r1; s >= r0; --s) {
-        const T cls = fac[lay.cell(1, colour, s, t)];
-        const T v = s == r1 ? fac[lay.cell(2, colour, s, t)]
-                            : fac[lay.cell(2, colour, s, t)] - cls * next_v;
-        const T w = s == r1 ? c_last / fac[lay.cell(0, colour, s, t)] : -cls * next_w;
-        fac[lay.cell(2, colour, s, t)] = v;
-        fac[lay.cell(3, colour, s, t)] = w;
-        next_v = v;
-        next_w = w;
-      }
+    double prev_u = 0.0;
+    for (int s = 0; s < extent; ++s) {
+      const int c = base + s * stride;
+      int i, j, k;
+      line_cell(axis, fa, fb, s, i, j, k);
+      T lowf, highf;
+      line_faces(L, axis, c, j, k, lowf, highf);
+      const double a = s == 0 ? 0.0 : -static_cast<double>(lowf);
+      const double cc = s + 1 == extent ? 0.0 : -static_cast<double>(highf);
+      const double den = static_cast<double>(L.diag[c]) - a * prev_u;
+      const double u = cc / den;
+      fac[lay.cell(0, colour, s, t)] = static_cast<T>(1.0 / den);
+      fac[lay.cell(1, colour, s, t)] = static_cast<T>(a / den);
+      fac[lay.cell(2, colour, s, t)] = static_cast<T>(u);
+      prev_u = u;
     }
-    // Interface matrix M u = y_I with u = (F_0, L_0, ..., F_{S-1}, L_{S-1}):
-    //   F_q + v_{r0} L_{q-1} + w_{r0} F_{q+1} = y_{r0}
-    //   L_q + v_{r1} L_{q-1} + w_{r1} F_{q+1} = y_{r1}
-    T m[4 * kMaxSegments * kMaxSegments];
-    T inv[4 * kMaxSegments * kMaxSegments];
-    for (int e = 0; e < n2 * n2; ++e) {
-      m[e] = T(0);
-      inv[e] = T(0);
-    }
-    for (int q = 0; q < S; ++q) {
-      int r0, r1;
-      segment_rows(extent, S, q, r0, r1);
-      const int rf = 2 * q, rl = 2 * q + 1;
-      m[rf * n2 + rf] = T(1);
-      m[rl * n2 + rl] = T(1);
-      if (q > 0) {
-        m[rf * n2 + 2 * (q - 1) + 1] += fac[lay.cell(2, colour, r0, t)];
-        m[rl * n2 + 2 * (q - 1) + 1] += fac[lay.cell(2, colour, r1, t)];
-      }
-      if (q + 1 < S) {
-        m[rf * n2 + 2 * (q + 1)] += fac[lay.cell(3, colour, r0, t)];
-        m[rl * n2 + 2 * (q + 1)] += fac[lay.cell(3, colour, r1, t)];
-      }
-    }
-    for (int e = 0; e < n2; ++e) inv[e * n2 + e] = T(1);
-    // Gauss-Jordan with partial pivoting (2S <= 16 unknowns).
-    for (int col = 0; col < n2; ++col) {
-      int piv = col;
-      T best = fabs(static_cast<double>(m[col * n2 + col]));
-      for (int r = col + 1; r < n2; ++r) {
-        const T mag = fabs(static_cast<double>(m[r * n2 + col]));
-        if (mag > best) {
-          best = mag;
-          piv = r;
-        }
-      }
-      if (piv != col) {
-        for (int e = 0; e < n2; ++e) {
-          T tmp = m[col * n2 + e]; m[col * n2 + e] = m[piv * n2 + e]; m[piv * n2 + e] = tmp;
-          tmp = inv[col * n2 + e]; inv[col * n2 + e] = inv[piv * n2 + e]; inv[piv * n2 + e] = tmp;
-        }
-      }
-      const T p = m[col * n2 + col];
-      for (int e = 0; e < n2; ++e) {
-        m[col * n2 + e] /= p;
-        inv[col * n2 + e] /= p;
-      }
-      for (int r = 0; r < n2; ++r) {
-        if (r == col) continue;
-        const T f = m[r * n2 + col];
-        if (f == T(0)) continue;
-        for (int e = 0; e < n2; ++e) {
-          m[r * n2 + e] -= f * m[col * n2 + e];
-          inv[r * n2 + e] -= f * inv[col * n2 + e];
-        }
-      }
-    }
-    for (int r = 0; r < n2; ++r)
-      for (int c = 0; c < n2; ++c) rinv[lay.rinv(n2, r, c, colour, t)] = inv[r * n2 + c];
   }
 }
 
-// One zebra colour with the partition method: blockDim = (32 lines, S).
-template <class T, int AXIS, int S>
-__global__ void __launch_bounds__(32 * S)
-    k_line_segment_color(Level<T> L, T* __restrict__ x,
-                         const T* __restrict__ rhs, const T* __restrict__ fac,
-                         int color) {
-  extern __shared__ unsigned char segment_smem[];
-  T* Y = reinterpret_cast<T*>(segment_smem);           // [extent][32]
+// One zebra colour: blockDim = (LPB lines, S chunks), chunk q holds rows
+// [q*m, min(extent, (q+1)*m) - 1] with m <= ScanConfig<T>::rows.  Shared memory holds
+// the chunk compositions: forward (A, B) and backward (A, B), S x LPB each.
+template <class T, int AXIS, int LPB>
+__global__ void __launch_bounds__(ScanConfig<T>::threads)
+    k_line_scan_color(Level<T> L, T* x, const T* __restrict__ rhs,
+                      const T* __restrict__ fac, int color, int m) {
+  extern __shared__ unsigned char scan_smem[];
+  const int S = blockDim.y;
+  T* fA = reinterpret_cast<T*>(scan_smem);
+  T* fB = fA + S * LPB;
+  T* bA = fB + S * LPB;
+  T* bB = bA + S * LPB;
   const int extent = line_extent(AXIS, L.nx, L.ny, L.nz);
-  T* UI = Y + static_cast<size_t>(extent) * kLanes;     // [2S][32]
-  T* YI = UI + 2 * S * kLanes;                          // [2S][32]
   const int a_extent = AXIS == 0 ? L.ny : L.nx;
   const int b_extent = AXIS == 2 ? L.ny : L.nz;
   const int ha = (a_extent + 1) >> 1;
-  const SegmentLayout lay{extent, ha * b_extent};
-  const T* rinv = fac + lay.cell_values();
+  const ScanLayout lay{extent, ha * b_extent};
   const int lane = threadIdx.x;
   const int q = threadIdx.y;
-  const int t = blockIdx.x * kLanes + lane;
+  const int t = blockIdx.x * LPB + lane;
   const int fb = t / ha;
   const int fa = 2 * (t - fb * ha) + ((fb + color) & 1);
   const bool valid = t < ha * b_extent && fa < a_extent;
   int base = 0, stride = 0;
   if (valid) line_geometry(L, AXIS, fa, fb, base, stride);
-  int r0, r1;
-  segment_rows(extent, S, q, r0, r1);
-  const T* den = fac + lay.cell(0, color, 0, t);
-  const T* cl = fac + lay.cell(1, color, 0, t);
-  const T* vv = fac + lay.cell(2, color, 0, t);
-  const T* ww = fac + lay.cell(3, color, 0, t);
-  const T* aa = fac + lay.cell(4, color, 0, t);
-  const size_t row = static_cast<size_t>(lay.colour_lines);
-  // Forward local elimination y' = (d - a y'_prev) / den, loads in chunks.
-  if (valid) {
-    T prev = T(0);
-    for (int s0 = r0; s0 <= r1; s0 += kChunk) {
-      T dv[kChunk], av[kChunk], dn[kChunk];
+  const int r0 = q * m;
+  const int rows = valid ? max(0, min(m, extent - r0)) : 0;
+  const int row = lay.colour_lines;
+  const int tt = valid ? t : 0;
+  const T* inv = fac + lay.cell(0, color, 0, tt);
+  const T* lf = fac + lay.cell(1, color, 0, tt);
+  const T* uf = fac + lay.cell(2, color, 0, tt);
+  // Rows past the chunk's end (padding, and every row of an idle thread)
+  // re-read the line's last row so that all loads are unconditional; their
+  // values are never used.
+  const auto srow = [&](int u) { return min(r0 + u, extent - 1); };
+
+  // Pass 1: right-hand sides scaled by 1/den, and the forward composition.
+  const LineRhs<T, AXIS> lr(L, valid ? fa : 0, valid ? fb : 0);
+  constexpr int kScanRows = ScanConfig<T>::rows;
+  T v[kScanRows];
 #pragma unroll
-      for (int u = 0; u < kChunk; ++u) {
-        const int s = s0 + u;
-        if (s <= r1) {
-          av[u] = aa[s * row];
-          dn[u] = den[s * row];
-          dv[u] = line_rhs<T, AXIS>(L, x, rhs, fa, fb, s, extent, base + s * stride);
-        }
-      }
+  for (int u = 0; u < kScanRows; ++u)
+    v[u] = lr.row(x, rhs, base + srow(u) * stride, srow(u), extent) * __ldg(inv + srow(u) * row);
+  T A = T(1), B = T(0);
 #pragma unroll
-      for (int u = 0; u < kChunk; ++u) {
-        const int s = s0 + u;
-        if (s <= r1) {
-          const T v = s == r0 ? dv[u] / dn[u] : (dv[u] - av[u] * prev) / dn[u];
-          Y[s * kLanes + lane] = v;
-          prev = v;
-        }
-      }
-    }
-    T next = T(0);
-    for (int s = r1; s >= r0; --s) {
-      const T yp = Y[s * kLanes + lane];
-      const T v = s == r1 ? yp : yp - cl[s * row] * next;
-      Y[s * kLanes + lane] = v;
-      next = v;
-    }
-    YI[(2 * q) * kLanes + lane] = Y[r0 * kLanes + lane];
-    YI[(2 * q + 1) * kLanes + lane] = Y[r1 * kLanes + lane];
+  for (int u = 0; u < kScanRows; ++u) {
+    const T l = __ldg(lf + srow(u) * row);
+    const bool on = u < rows;
+    B = on ? v[u] - l * B : B;
+    A = on ? -l * A : A;
   }
+  fA[q * LPB + lane] = A;
+  fB[q * LPB + lane] = B;
   __syncthreads();
-  // Interface unknowns F_q, L_q = rows 2q, 2q+1 of R applied to y_I.
-  if (valid) {
-    constexpr int n2 = 2 * S;
-    T f = T(0), l = T(0);
+  // Forward replay from y_{r0-1}.
+  T y = T(0);
+  for (int p = 0; p < q; ++p) y = fA[p * LPB + lane] * y + fB[p * LPB + lane];
 #pragma unroll
-    for (int e = 0; e < n2; ++e) {
-      const T y = YI[e * kLanes + lane];
-      f += rinv[lay.rinv(n2, 2 * q, e, color, t)] * y;
-      l += rinv[lay.rinv(n2, 2 * q + 1, e, color, t)] * y;
-    }
-    UI[(2 * q) * kLanes + lane] = f;
-    UI[(2 * q + 1) * kLanes + lane] = l;
+  for (int u = 0; u < kScanRows; ++u) {
+    y = v[u] - __ldg(lf + srow(u) * row) * y;
+    v[u] = y;
   }
+  // Backward composition x_{r0} = A x_{r1+1} + B.
+  A = T(1);
+  B = T(0);
+#pragma unroll
+  for (int u = kScanRows - 1; u >= 0; --u) {
+    const T uu = __ldg(uf + srow(u) * row);
+    const bool on = u < rows;
+    B = on ? v[u] - uu * B : B;
+    A = on ? -uu * A : A;
+  }
+  bA[q * LPB + lane] = A;
+  bB[q * LPB + lane] = B;
   __syncthreads();
-  if (valid) {
-    const T left = q > 0 ? UI[(2 * (q - 1) + 1) * kLanes + lane] : T(0);
-    const T right = q + 1 < S ? UI[(2 * (q + 1)) * kLanes + lane] : T(0);
-    for (int s = r0; s <= r1; ++s)
-      x[base + s * stride] = Y[s * kLanes + lane] - vv[s * row] * left - ww[s * row] * right;
+  T xn = T(0);
+  for (int p = S - 1; p > q; --p) xn = bA[p * LPB + lane] * xn + bB[p * LPB + lane];
+#pragma unroll
+  for (int u = kScanRows - 1; u >= 0; --u) {
+    const T xv = v[u] - __ldg(uf + srow(u) * row) * xn;
+    xn = u < rows ? xv : xn;
+    if (u < rows) x[base + srow(u) * stride] = xn;
   }
 }
 
@@ -606,23 +631,43 @@ void pcr_shape(int extent, int& P, int& lines_per_block, int& steps) {
   lines_per_block = std::max(1, std::min(1024 / P, 4));
 }
 
-template <class T, int AXIS, int S>
-void launch_segment(cudaStream_t s, const Level<T>& L, T* x, const T* b,
-                    const T* fac, int color, int blocks, size_t smem) {
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_line_segment_color<T, AXIS, S>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-  k_line_segment_color<T, AXIS, S><<<blocks, dim3(kLanes, S), smem, s>>>(L, x, b, fac, color);
+// Lines per block and chunks per line of the scan kernel: at least 296
+// blocks (two per SM) where the level allows, at most ScanConfig<T>::threads
+// threads, at least 8 lines per block while that still allows chunks of at
+// most ScanConfig<T>::rows rows.
+struct ScanShape {
+  int lpb, chunks, rows;
+};
+
+template <class T>
+ScanShape scan_shape(long long per_color, int extent) {
+  constexpr int rows = ScanConfig<T>::rows;
+  ScanShape sh{32, (extent + rows - 1) / rows, 0};
+  while (sh.lpb > 8 && per_color < 296LL * sh.lpb) sh.lpb >>= 1;
+  while (sh.lpb > 1 && sh.lpb * sh.chunks > ScanConfig<T>::threads) sh.lpb >>= 1;
+  sh.rows = (extent + sh.chunks - 1) / sh.chunks;
+  return sh;
+}
+
+template <class T, int AXIS, int LPB>
+void launch_scan(cudaStream_t s, const Level<T>& L, T* x, const T* b, const T* fac,
+                 int color, long long per_color, const ScanShape& sh) {
+  const int blocks = static_cast<int>((per_color + LPB - 1) / LPB);
+  const size_t smem = static_cast<size_t>(4) * sh.chunks * LPB * sizeof(T);
+  k_line_scan_color<T, AXIS, LPB><<<blocks, dim3(LPB, sh.chunks), smem, s>>>(L, x, b, fac, color,
+                                                                             sh.rows);
 }
 
 template <class T, int AXIS>
-void launch_segment_axis(cudaStream_t s, const Level<T>& L, T* x, const T* b,
-                         const T* fac, int color, int S, int blocks, size_t smem) {
-  switch (S) {
-    case 1: launch_segment<T, AXIS, 1>(s, L, x, b, fac, color, blocks, smem); break;
-    case 2: launch_segment<T, AXIS, 2>(s, L, x, b, fac, color, blocks, smem); break;
-    case 4: launch_segment<T, AXIS, 4>(s, L, x, b, fac, color, blocks, smem); break;
-    default: launch_segment<T, AXIS, 8>(s, L, x, b, fac, color, blocks, smem); break;
+void launch_scan_axis(cudaStream_t s, const Level<T>& L, T* x, const T* b, const T* fac,
+                      int color, long long per_color, const ScanShape& sh) {
+  switch (sh.lpb) {
+    case 32: launch_scan<T, AXIS, 32>(s, L, x, b, fac, color, per_color, sh); break;
+    case 16: launch_scan<T, AXIS, 16>(s, L, x, b, fac, color, per_color, sh); break;
+    case 8: launch_scan<T, AXIS, 8>(s, L, x, b, fac, color, per_color, sh); break;
+    case 4: launch_scan<T, AXIS, 4>(s, L, x, b, fac, color, per_color, sh); break;
+    case 2: launch_scan<T, AXIS, 2>(s, L, x, b, fac, color, per_color, sh); break;
+    default: launch_scan<T, AXIS, 1>(s, L, x, b, fac, color, per_color, sh); break;
   }
 }
 
@@ -634,7 +679,7 @@ int line_kind(int nx, int ny, int nz, int axis) {
   const int b_extent = axis == 2 ? ny : nz;
   const long long per_color = static_cast<long long>((a_extent + 1) / 2) * b_extent;
   if (per_color < kLinePcrThreshold && extent <= 1024) return kLinePcr;
-  return kLineSegment;
+  return extent <= kScanMaxExtent ? kLineScan : kLineNone;
 }
 
 size_t line_factor_values(int nx, int ny, int nz, int axis) {
@@ -642,12 +687,9 @@ size_t line_factor_values(int nx, int ny, int nz, int axis) {
   const int a_extent = axis == 0 ? ny : nx;
   const int b_extent = axis == 2 ? ny : nz;
   const size_t lines = static_cast<size_t>(a_extent) * b_extent;
-  if (line_kind(nx, ny, nz, axis) == kLineSegment) {
-    const size_t S = static_cast<size_t>(segments_for(extent));
-    const SegmentLayout lay{extent, ((a_extent + 1) / 2) * b_extent};
-    // 5 colour-packed arrays per row, plus the interface inverse per line.
-    return lay.cell_values() + 2 * static_cast<size_t>(lay.colour_lines) * 4 * S * S;
-  }
+  const int kind = line_kind(nx, ny, nz, axis);
+  if (kind == kLineNone) return 0;
+  if (kind == kLineScan) return ScanLayout{extent, ((a_extent + 1) / 2) * b_extent}.values();
   int P, lpb, steps;
   pcr_shape(extent, P, lpb, steps);
   return static_cast<size_t>(2 * steps + 1) * lines * P;
@@ -659,9 +701,10 @@ void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac) {
   const int a_extent = axis == 0 ? L.ny : L.nx;
   const int b_extent = axis == 2 ? L.ny : L.nz;
   const int lines = a_extent * b_extent;
-  if (line_kind(L.nx, L.ny, L.nz, axis) == kLineSegment) {
-    const int S = segments_for(extent);
-    k_segment_factors<T><<<(lines + 63) / 64, 64, 0, s>>>(L, axis, S, fac);
+  const int kind = line_kind(L.nx, L.ny, L.nz, axis);
+  if (kind == kLineNone) return;
+  if (kind == kLineScan) {
+    k_scan_factors<T><<<(lines + 127) / 128, 128, 0, s>>>(L, axis, fac);
     return;
   }
   int P, lpb, steps;
@@ -678,13 +721,13 @@ void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
   const int a_extent = axis == 0 ? L.ny : L.nx;
   const int b_extent = axis == 2 ? L.ny : L.nz;
   const long long per_color = static_cast<long long>((a_extent + 1) / 2) * b_extent;
-  if (line_kind(L.nx, L.ny, L.nz, axis) == kLineSegment) {
-    const int S = segments_for(extent);
-    const int blocks = static_cast<int>((per_color + kLanes - 1) / kLanes);
-    const size_t smem = (static_cast<size_t>(extent) + 4 * S) * kLanes * sizeof(T);
-    if (axis == 0) launch_segment_axis<T, 0>(s, L, x, b, fac, color, S, blocks, smem);
-    else if (axis == 1) launch_segment_axis<T, 1>(s, L, x, b, fac, color, S, blocks, smem);
-    else launch_segment_axis<T, 2>(s, L, x, b, fac, color, S, blocks, smem);
+  const int kind = line_kind(L.nx, L.ny, L.nz, axis);
+  if (kind == kLineNone) return;
+  if (kind == kLineScan) {
+    const ScanShape sh = scan_shape<T>(per_color, extent);
+    if (axis == 0) launch_scan_axis<T, 0>(s, L, x, b, fac, color, per_color, sh);
+    else if (axis == 1) launch_scan_axis<T, 1>(s, L, x, b, fac, color, per_color, sh);
+    else launch_scan_axis<T, 2>(s, L, x, b, fac, color, per_color, sh);
     return;
   }
   int P, lpb, steps;

@@ -204,6 +204,10 @@ Status Solver::create(const hfps_geometry& g, const hfps_policy& policy,
 Status Solver::allocate() {
   const std::vector<Shape> shapes = level_shapes(faces_, policy_);
   if (shapes.size() < 2) return fail(HFPS_INVALID_PLAN, kDetailPlan, "fewer than two levels");
+  for (const Shape& s : shapes)
+    for (int a = 0; a < 3; ++a)
+      if ((s.line_mask & (1 << a)) && line_kind(s.n[0], s.n[1], s.n[2], a) == kLineNone)
+        return fail(HFPS_INVALID_PLAN, kDetailPlan, "line relaxation: line longer than 2048 cells");
   const int levels = static_cast<int>(shapes.size());
   // Sizes.
   size_t bytes = 0;

@@ -4,7 +4,7 @@ Bars:
 * level coefficients and point-smoother MG corrections (red-black,
   Chebyshev, V and F cycles): bit-identical to the C restatement, which is
   itself bit-identical to the reference;
-* line relaxation (partition method on large levels, PCR on small ones):
+* line relaxation (chunked scan on large levels, PCR on small ones):
   1e-11 relative;
 * exact operator: 1e-15 relative (IBM faces folded into the coefficients
   instead of applied as link corrections);
@@ -90,12 +90,13 @@ def test_mg_correction_matches(hfps_mod, name):
         assert np.array_equal(z, golden_cases.arrays(name)["mg"])
 
 
-def test_mg_segmented_lines_match(hfps_mod):
-    """Line colours with many lines use the partition method (segments per
-    warp, spikes, interface inverse): the zebra cycle matches the
-    restatement's serial Thomas solves to rounding."""
+@pytest.mark.parametrize("shape", [(128, 96, 96), (73, 150, 40)])
+def test_mg_scan_lines_match(hfps_mod, shape):
+    """Line colours with many lines use the chunked-scan solve (chunks of 16
+    rows per thread combined through shared memory): the zebra cycle matches
+    the restatement's serial Thomas solves to rounding."""
     import ref_oracle
-    s = workloads.make("wrinkled256", n=(128, 96, 96), stretch_y=1.05, seed=4)
+    s = workloads.make("wrinkled256", n=shape, stretch_y=1.05, seed=4)
     pol = ref_oracle.MgPolicy(cycle=0, pre=1, post=1, coarse_sweeps=2, max_levels=2)
     g = hfps_mod.PressureSolver.from_system(s, gpu_policy(hfps_mod, pol))
     o = oracle(s, pol, line_order=1)
