@@ -73,11 +73,14 @@ def barrier(world):
 
 
 def max_over_ranks(world, value):
+    """Slowest rank's time: replicas are timed on their own devices and the
+    job takes as long as its slowest rank."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -173,33 +176,100 @@ class ReferenceSampler:
         self.session.close()
 
 
+def _reference_worker(shape, iterations, steps, start, conn):
+    """One replica of the reference solve on one host core (spawned)."""
+    try:
+        os.environ["OMP_NUM_THREADS"] = "1"
+        from hfps import workloads
+        system = workloads.make(CONFIG_NAME, **({"n": tuple(shape)} if shape else {}))
+        sampler = ReferenceSampler(system)
+        kind = sampler.kind
+        del system
+        times = []
+        for _ in range(steps):
+            start.wait()
+            times.append(sampler.seconds_per_iteration(iterations))
+        sampler.close()
+        conn.send(("ok", kind, times))
+    except BaseException as exc:  # report, never hang the parent
+        conn.send(("error", repr(exc), []))
+    finally:
+        conn.close()
+
+
+def reference_workers():
+    """Host cores to use, bounded by memory: a 256^3 replica of the
+    reference solver peaks near 5.5 GB of host memory."""
+    cores = len(os.sched_getaffinity(0))
+    available = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    available = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    if available is None:
+        return 1
+    return max(1, min(cores, int(0.5 * available / 6.5e9)))
+
+
+def time_reference_parallel(args, workers, iterations, steps):
+    """Runs `workers` independent single-threaded replicas of the reference
+    solve, one per core, each timing `steps` samples of `iterations` PCG
+    iterations in lock-step; returns (kind, solves/s summed over replicas
+    per step)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    start = ctx.Barrier(workers)
+    pipes, procs = [], []
+    for _ in range(workers):
+        parent, child = ctx.Pipe(duplex=False)
+        p = ctx.Process(target=_reference_worker,
+                        args=(args.shape, iterations, steps, start, child))
+        p.start()
+        child.close()
+        pipes.append(parent)
+        procs.append(p)
+    results = [c.recv() for c in pipes]
+    for p in procs:
+        p.join()
+    errors = [r[1] for r in results if r[0] != "ok"]
+    if errors:
+        raise RuntimeError(f"reference replica failed: {errors[0]}")
+    kind = results[0][1]
+    per_step = []
+    for k in range(steps):
+        per_step.append(sum(1.0 / (r[2][k] * REFERENCE_ITERATIONS_PER_SOLVE) for r in results))
+    return kind, per_step, [r[2] for r in results]
+
+
 def run_reference(args, world, rank):
-    """The reference arm: the reference's own CPU MG-PCG on this workload."""
+    """The reference arm: the reference's own CPU MG-PCG (solve_pcg +
+    NativeCartesianMgPlan compiled from its sources) on this workload, one
+    single-threaded replica per host core; the solve of one system is
+    single-threaded in the reference (one MPI rank)."""
     if rank != 0:
         return
-    system = make_system(args)
-    sampler = ReferenceSampler(system)
-    kind = sampler.kind
-    per_iteration = []
-    for step in range(args.warmup + args.steps):
-        seconds = sampler.seconds_per_iteration(1)
-        if step >= args.warmup:
-            per_iteration.append(seconds)
-    sampler.close()
-    t_iter = statistics.mean(per_iteration)
-    iterations = REFERENCE_ITERATIONS_PER_SOLVE
-    value = 1.0 / (t_iter * iterations)
+    workers = reference_workers()
+    kind, per_step, raw = time_reference_parallel(args, workers, 1, args.warmup + args.steps)
+    timed = per_step[args.warmup:]
+    value = statistics.mean(timed)
+    t_iter = statistics.mean(t for r in raw for t in r[args.warmup:])
+    shape = list(args.shape) if args.shape else [256, 256, 256]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
-        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64/Box-Muller)",
-        "config": {"workload": "wrinkled256 warm-start pressure solve", "shape": list(system.shape),
+        "config": {"workload": "wrinkled256 warm-start pressure solve (256^3 stretched)",
+                   "shape": shape,
                    "algorithm": "solve_pcg + NativeCartesianMgPlan (production policy, unit_linear)",
                    "rtol": RTOL},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
-                         "sample": f"{args.steps} x 1 PCG iteration of the 256^3 system "
-                                   f"({t_iter:.2f} s each) x {iterations} iterations per solve"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": kind,
+                         "sample": f"{workers} single-threaded replicas x 1 PCG iteration per step "
+                                   f"({t_iter:.2f} s each) x {REFERENCE_ITERATIONS_PER_SOLVE} "
+                                   f"iterations per solve, summed over replicas"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -316,14 +386,13 @@ def run_b200(args, world, rank, local):
     iterations = [i["iterations"] for i in infos]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sampler = ReferenceSampler(system)
-        kind = sampler.kind
-        t_iter = sampler.seconds_per_iteration(2)
-        sampler.close()
-        cpu = {"value": 1.0 / (t_iter * REFERENCE_ITERATIONS_PER_SOLVE), "unit": UNIT, "cores": 1,
-               "kind": kind,
-               "sample": f"2 PCG iterations of the 256^3 system ({t_iter:.2f} s each) x "
-                         f"{REFERENCE_ITERATIONS_PER_SOLVE} iterations per solve"}
+        workers = reference_workers()
+        kind, per_step, raw = time_reference_parallel(args, workers, 1, 2)
+        t_iter = statistics.mean(t for r in raw for t in r)
+        cpu = {"value": statistics.mean(per_step), "unit": UNIT, "cores": workers, "kind": kind,
+               "sample": f"{workers} single-threaded replicas x 2 PCG iterations of the 256^3 "
+                         f"system ({t_iter:.2f} s each) x {REFERENCE_ITERATIONS_PER_SOLVE} "
+                         f"iterations per solve, summed over replicas"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -16,7 +16,54 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+// Programmatic dependent launch: every kernel of the library is launched
+// with programmatic stream serialisation (hfps::launch), so the launch of
+// the next kernel in a stream or graph overlaps the drain of this one.  Each
+// kernel therefore starts with grid_dependency_sync(), which waits until the
+// preceding grid has completed and its writes are visible, before touching
+// any memory.  Kernels launched without the attribute pass it straight
+// through.  An early launch_dependents trigger (dependents scheduled while
+// this grid still runs) measured 3% faster on the FP64 MG cycle but 7%
+// slower on the FP32 one at 256^3, so dependents launch at grid exit.
+#ifndef HFPS_USE_PDL
+#define HFPS_USE_PDL 1
+#endif
+#ifndef HFPS_PDL_EARLY_TRIGGER
+#define HFPS_PDL_EARLY_TRIGGER 0
+#endif
+
 namespace hfps {
+
+__device__ __forceinline__ void grid_dependency_sync() {
+#if HFPS_USE_PDL
+#if HFPS_PDL_EARLY_TRIGGER
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#endif
+}
+
+// Launches kernel<<<grid, block, smem, stream>>>(args...) with programmatic
+// stream serialisation allowed.
+template <class... Params, class... Args>
+inline void launch(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem,
+                   cudaStream_t stream, Args&&... args) {
+#if HFPS_USE_PDL
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+#else
+  kernel<<<grid, block, smem, stream>>>(static_cast<Params>(args)...);
+#endif
+}
 
 // Bit f of `neumann` is set when face f (x-,x+,y-,y+,z-,z+) is Neumann; a
 // clear bit is Dirichlet (neighbour value 0).  Neumann reads the cell

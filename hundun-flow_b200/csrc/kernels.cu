@@ -109,6 +109,7 @@ __device__ __forceinline__ void cell_coords(int c, int nx, int ny, int& i,
 template <class T>
 __global__ void k_level_apply(Level<T> L, const T* __restrict__ x,
                               T* __restrict__ y) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -121,6 +122,7 @@ __global__ void k_level_apply(Level<T> L, const T* __restrict__ x,
 template <class T>
 __global__ void k_level_defect(Level<T> L, const T* __restrict__ x,
                                const T* __restrict__ b, T* __restrict__ r) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -137,6 +139,7 @@ __global__ void k_level_defect(Level<T> L, const T* __restrict__ x,
 template <class T>
 __global__ void k_rb_color(Level<T> L, T* __restrict__ x,
                            const T* __restrict__ b, int color) {
+  grid_dependency_sync();
   const int hx = (L.nx + 1) >> 1;
   const int n = hx * L.ny * L.nz;
   const T omega = T(0.72);
@@ -162,6 +165,7 @@ __global__ void k_chebyshev_stage(Level<T> L, const T* __restrict__ x,
                                   T* __restrict__ direction,
                                   T* __restrict__ next, T previous_factor,
                                   T residual_factor, int first) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -249,6 +253,7 @@ __global__ void k_defect_restrict(Level<T> F, const T* __restrict__ x,
                                   const T* __restrict__ b, Level<T> C,
                                   T* __restrict__ cb, T* __restrict__ cx,
                                   int mask) {
+  grid_dependency_sync();
   const int n = C.nx * C.ny * C.nz;
   const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
   for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
@@ -273,6 +278,7 @@ __global__ void k_defect_restrict(Level<T> F, const T* __restrict__ x,
 template <class T>
 __global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
                            T* __restrict__ cb, T* __restrict__ cx, int mask) {
+  grid_dependency_sync();
   const int n = C.nx * C.ny * C.nz;
   const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
   for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
@@ -323,41 +329,55 @@ __device__ __forceinline__ void interp_axis(int fine, int coarsened,
 // Trilinear prolongation and add, zero on solid cells (prolongate_add,
 // src/solver_mg.cpp:3893-3994).  Weights are formed in double exactly as
 // the reference does and rounded once to T for the FP32 hierarchy.
+//
+// One fine cell per thread, branch-free: the up to 2x2x2 coarse candidates
+// are loaded unconditionally (a degenerate axis repeats its one index) and
+// the terms are added in the reference's order (z outer, x inner) with the
+// absent ones skipped by selects, so the sum is the reference's bit for bit
+// while all loads of a cell are in flight together.
 template <class T>
 __global__ void k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C,
                              const T* __restrict__ cx, int mask) {
+  grid_dependency_sync();
   const int n = F.nx * F.ny * F.nz;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
   const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
-    if (F.fluid[c] == 0) {
-      x[c] = T(0);
-      continue;
-    }
-    int i, j, k;
-    cell_coords(c, F.nx, F.ny, i, j, k);
-    int xl, xr, yl, yr, zl, zr;
-    double xw, yw, zw;
-    interp_axis(i, mx, C.nx, xl, xr, xw);
-    interp_axis(j, my, C.ny, yl, yr, yw);
-    interp_axis(k, mz, C.nz, zl, zr, zw);
-    T value = T(0);
-    for (int az = 0; az < (zl == zr ? 1 : 2); ++az) {
-      const int gz = az == 0 ? zl : zr;
-      const double wz = az == 0 ? 1.0 - zw : zw;
-      for (int ay = 0; ay < (yl == yr ? 1 : 2); ++ay) {
-        const int gy = ay == 0 ? yl : yr;
+  const bool fluid = F.fluid[c] != 0;
+  const T old = x[c];
+  int i, j, k;
+  cell_coords(c, F.nx, F.ny, i, j, k);
+  int xi[2], yi[2], zi[2];
+  double xw, yw, zw;
+  interp_axis(i, mx, C.nx, xi[0], xi[1], xw);
+  interp_axis(j, my, C.ny, yi[0], yi[1], yw);
+  interp_axis(k, mz, C.nz, zi[0], zi[1], zw);
+  const bool two_x = xi[0] != xi[1], two_y = yi[0] != yi[1], two_z = zi[0] != zi[1];
+  T term[2][2][2];
+#pragma unroll
+  for (int az = 0; az < 2; ++az)
+#pragma unroll
+    for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+      for (int ax = 0; ax < 2; ++ax) {
+        const double wz = az == 0 ? 1.0 - zw : zw;
         const double wy = ay == 0 ? 1.0 - yw : yw;
-        for (int ax = 0; ax < (xl == xr ? 1 : 2); ++ax) {
-          const int gx = ax == 0 ? xl : xr;
-          const double wx = ax == 0 ? 1.0 - xw : xw;
-          const T w = static_cast<T>(wx * wy * wz);
-          value += w * cx[gx + C.nx * (gy + C.ny * gz)];
-        }
+        const double wx = ax == 0 ? 1.0 - xw : xw;
+        const T w = static_cast<T>(wx * wy * wz);
+        term[az][ay][ax] = w * __ldg(cx + xi[ax] + C.nx * (yi[ay] + C.ny * zi[az]));
       }
-    }
-    x[c] += value;
-  }
+  T value = T(0);
+#pragma unroll
+  for (int az = 0; az < 2; ++az)
+#pragma unroll
+    for (int ay = 0; ay < 2; ++ay)
+#pragma unroll
+      for (int ax = 0; ax < 2; ++ax) {
+        const bool on = (az == 0 || two_z) && (ay == 0 || two_y) && (ax == 0 || two_x);
+        const T sum = value + term[az][ay][ax];
+        value = on ? sum : value;
+      }
+  x[c] = fluid ? old + value : T(0);
 }
 
 // Coarsest level: `sweeps` smoother sweeps in one CTA (mg_cycle coarse
@@ -368,6 +388,7 @@ template <class T, class TC>
 __global__ void k_coarse_solve(Level<TC> L, T* x, const T* b, TC* xs, TC* bs,
                                TC* work, TC* dprime, int sweeps,
                                int line_axis) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   TC* xw = xs;
   const TC* bw = bs;
@@ -429,6 +450,7 @@ template <class T>
 __global__ void k_mg_enter(int n, const double* __restrict__ r,
                            const uint8_t* __restrict__ active,
                            T* __restrict__ b, T* __restrict__ x) {
+  grid_dependency_sync();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
     const bool on = active == nullptr || active[c] != 0;
@@ -442,6 +464,7 @@ __global__ void k_mg_exit(int n, const T* __restrict__ x,
                           const uint8_t* __restrict__ active,
                           const double* __restrict__ scale_ptr,
                           double* __restrict__ z) {
+  grid_dependency_sync();
   const double scale = scale_ptr == nullptr ? 1.0 : *scale_ptr;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -454,6 +477,7 @@ template <class T>
 __global__ void k_diagonal_solve(int n, const T* __restrict__ b,
                                  const T* __restrict__ diag,
                                  T* __restrict__ x) {
+  grid_dependency_sync();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x)
     x[c] = b[c] / diag[c];
@@ -463,6 +487,7 @@ template <class T>
 __global__ void k_mg_projection(int n, const double* __restrict__ r_in,
                                 const uint8_t* __restrict__ active,
                                 const T* __restrict__ recursive, Reduce red) {
+  grid_dependency_sync();
   double v[3] = {0.0, 0.0, 0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -492,6 +517,7 @@ __global__ void k_mg_projection(int n, const double* __restrict__ r_in,
 // (:1448-1463), r.z (:1536-1540) and p = z + beta p (:1546).
 __global__ void k_spmv_dot(Level<double> L, const double* __restrict__ x,
                            double* __restrict__ y, Reduce red) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   double v[1] = {0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
@@ -509,6 +535,7 @@ __global__ void k_spmv_dot(Level<double> L, const double* __restrict__ x,
 __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
                                 const double* __restrict__ b,
                                 double* __restrict__ r, Reduce red) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   double v[1] = {0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
@@ -527,6 +554,7 @@ __global__ void k_pcg_update(int n, double* __restrict__ x,
                              const double* __restrict__ p,
                              double* __restrict__ r,
                              const double* __restrict__ ap, Reduce red) {
+  grid_dependency_sync();
   const double alpha = red.scalars->alpha;
   double v[1] = {0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
@@ -542,6 +570,7 @@ __global__ void k_pcg_update(int n, double* __restrict__ x,
 
 __global__ void k_dot(int n, const double* __restrict__ a,
                       const double* __restrict__ b, Reduce red) {
+  grid_dependency_sync();
   double v[1] = {0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x)
@@ -551,6 +580,7 @@ __global__ void k_dot(int n, const double* __restrict__ a,
 }
 
 __global__ void k_norm2(int n, const double* __restrict__ a, Reduce red) {
+  grid_dependency_sync();
   double v[1] = {0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x)
@@ -562,6 +592,7 @@ __global__ void k_norm2(int n, const double* __restrict__ a, Reduce red) {
 __global__ void k_p_update(int n, double* __restrict__ p,
                            const double* __restrict__ z,
                            const Scalars* __restrict__ sc) {
+  grid_dependency_sync();
   const double beta = sc->beta;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x)
@@ -570,6 +601,7 @@ __global__ void k_p_update(int n, double* __restrict__ p,
 
 __global__ void k_copy(int n, const double* __restrict__ src,
                        double* __restrict__ dst) {
+  grid_dependency_sync();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x)
     dst[c] = src[c];
@@ -587,6 +619,7 @@ __global__ void k_mask_faces(int nx, int ny, int nz, const double* fx_in,
                              const double* fy_in, const double* fz_in,
                              const uint8_t* active, double* fx, double* fy,
                              double* fz) {
+  grid_dependency_sync();
   const int nfx = (nx + 1) * ny * nz;
   const int nfy = nx * (ny + 1) * nz;
   const int nfz = nx * ny * (nz + 1);
@@ -632,6 +665,7 @@ __global__ void k_mask_cells(int nx, int ny, int nz, const double* x_faces,
                              const double* fx, const double* fy,
                              const double* fz, double* volume,
                              uint8_t* fluid) {
+  grid_dependency_sync();
   const int n = nx * ny * nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -666,6 +700,7 @@ __global__ void k_mask_cells(int nx, int ny, int nz, const double* x_faces,
 // aggregated into the coarse diagonal (src/solver_mg.cpp:1880-1894).
 __global__ void k_reaction(Level<double> L, const double* volume,
                            double* reaction) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -691,6 +726,7 @@ __global__ void k_reaction(Level<double> L, const double* volume,
 __global__ void k_aggregate_axis(const double* src, int ex, int ey, int ez,
                                  double* dst, int dx, int dy, int dz, int axis,
                                  int face_axis, int global_extent) {
+  grid_dependency_sync();
   const int n = dx * dy * dz;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += gridDim.x * blockDim.x) {
@@ -721,6 +757,7 @@ __global__ void k_coarse_diagonal(int nx, int ny, int nz, double* diag,
                                   const double* fx, const double* fy,
                                   const double* fz, const double* volume,
                                   uint8_t* fluid) {
+  grid_dependency_sync();
   const int n = nx * ny * nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -742,6 +779,7 @@ __global__ void k_beta_faces(int nx, int ny, int nz, const double* xf,
                              const double* yf, const double* zf,
                              unsigned neumann, const double* beta, double* fx,
                              double* fy, double* fz) {
+  grid_dependency_sync();
   const int nfx = (nx + 1) * ny * nz;
   const int nfy = nx * (ny + 1) * nz;
   const int nfz = nx * ny * (nz + 1);
@@ -807,6 +845,7 @@ __global__ void k_beta_faces(int nx, int ny, int nz, const double* xf,
 __global__ void k_beta_diagonal(int nx, int ny, int nz, const double* fx,
                                 const double* fy, const double* fz,
                                 const double* storage, double* diag) {
+  grid_dependency_sync();
   const int n = nx * ny * nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
@@ -822,6 +861,7 @@ __global__ void k_beta_diagonal(int nx, int ny, int nz, const double* fx,
 }
 
 __global__ void k_shortcut_ratio(Level<double> L, Reduce red) {
+  grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   double v[1] = {0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
@@ -849,6 +889,7 @@ __global__ void k_shortcut_ratio(Level<double> L, Reduce red) {
 template <class TO, class TI>
 __global__ void k_convert(size_t n, const TI* __restrict__ src,
                           TO* __restrict__ dst) {
+  grid_dependency_sync();
   for (size_t c = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
        c < n; c += static_cast<size_t>(gridDim.x) * blockDim.x)
     dst[c] = static_cast<TO>(src[c]);
@@ -859,6 +900,7 @@ __global__ void k_convert(size_t n, const TI* __restrict__ src,
 __global__ void k_face_gradients(Level<double> L, const double* lambda,
                                  const double* p, double* gx, double* gy,
                                  double* gz) {
+  grid_dependency_sync();
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   const int nfx = (nx + 1) * ny * nz;
   const int nfy = nx * (ny + 1) * nz;
@@ -907,6 +949,7 @@ __global__ void k_face_gradients(Level<double> L, const double* lambda,
 
 __global__ void k_adjoint_source(int n, const double* dl_dp,
                                  const uint8_t* active, double* out) {
+  grid_dependency_sync();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x)
     out[c] = cell_on(active, c) ? dl_dp[c] : 0.0;
@@ -926,100 +969,102 @@ int reduction_blocks(long long items) {
 
 template <class T>
 void launch_level_apply(cudaStream_t s, const Level<T>& L, const T* x, T* y) {
-  k_level_apply<T><<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, y);
+  launch(k_level_apply<T>, grid_for(HFPS_CELLS(L)), kThreads, 0, s, L, x, y);
 }
 template <class T>
 void launch_level_defect(cudaStream_t s, const Level<T>& L, const T* x,
                          const T* b, T* r) {
-  k_level_defect<T><<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, b, r);
+  launch(k_level_defect<T>, grid_for(HFPS_CELLS(L)), kThreads, 0, s, L, x, b, r);
 }
 template <class T>
 void launch_rb_color(cudaStream_t s, const Level<T>& L, T* x, const T* b,
                      int color) {
   const long long half = static_cast<long long>((L.nx + 1) / 2) * L.ny * L.nz;
-  k_rb_color<T><<<grid_for(half), kThreads, 0, s>>>(L, x, b, color);
+  launch(k_rb_color<T>, grid_for(half), kThreads, 0, s, L, x, b, color);
 }
 template <class T>
 void launch_chebyshev_stage(cudaStream_t s, const Level<T>& L, const T* x,
                             const T* b, T* direction, T* next,
                             T previous_factor, T residual_factor, int first) {
-  k_chebyshev_stage<T><<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(
+  launch(k_chebyshev_stage<T>, grid_for(HFPS_CELLS(L)), kThreads, 0, s, 
       L, x, b, direction, next, previous_factor, residual_factor, first);
 }
 template <class T>
 void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
                             const T* b, const Level<T>& C, T* cb, T* cx,
                             int mask) {
-  k_defect_restrict<T><<<grid_for(HFPS_CELLS(C)), kThreads, 0, s>>>(F, x, b, C, cb,
+  launch(k_defect_restrict<T>, grid_for(HFPS_CELLS(C)), kThreads, 0, s, F, x, b, C, cb,
                                                                    cx, mask);
 }
 template <class T>
 void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
                      const Level<T>& C, T* cb, T* cx, int mask) {
-  k_restrict<T><<<grid_for(HFPS_CELLS(C)), kThreads, 0, s>>>(F, r, C, cb, cx, mask);
+  launch(k_restrict<T>, grid_for(HFPS_CELLS(C)), kThreads, 0, s, F, r, C, cb, cx, mask);
 }
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int mask) {
-  k_prolongate<T><<<grid_for(HFPS_CELLS(F)), kThreads, 0, s>>>(F, x, C, cx, mask);
+  const long long cells = HFPS_CELLS(F);
+  launch(k_prolongate<T>, static_cast<int>((cells + kThreads - 1) / kThreads), kThreads, 0, s, 
+      F, x, C, cx, mask);
 }
 template <class T, class TC>
 void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
                          TC* xs, TC* bs, TC* work, TC* dprime, int sweeps,
                          int line_axis) {
-  k_coarse_solve<T, TC><<<1, 512, 0, s>>>(L, x, b, xs, bs, work, dprime, sweeps,
+  launch(k_coarse_solve<T, TC>, 1, 512, 0, s, L, x, b, xs, bs, work, dprime, sweeps,
                                           line_axis);
 }
 template <class T>
 void launch_mg_enter(cudaStream_t s, int n, const double* r,
                      const uint8_t* active, T* b, T* x) {
-  k_mg_enter<T><<<grid_for(n), kThreads, 0, s>>>(n, r, active, b, x);
+  launch(k_mg_enter<T>, grid_for(n), kThreads, 0, s, n, r, active, b, x);
 }
 template <class T>
 void launch_mg_exit(cudaStream_t s, int n, const T* x, const uint8_t* active,
                     const double* scale_ptr, double* z) {
-  k_mg_exit<T><<<grid_for(n), kThreads, 0, s>>>(n, x, active, scale_ptr, z);
+  launch(k_mg_exit<T>, grid_for(n), kThreads, 0, s, n, x, active, scale_ptr, z);
 }
 template <class T>
 void launch_diagonal_solve(cudaStream_t s, int n, const T* b, const T* diag,
                            T* x) {
-  k_diagonal_solve<T><<<grid_for(n), kThreads, 0, s>>>(n, b, diag, x);
+  launch(k_diagonal_solve<T>, grid_for(n), kThreads, 0, s, n, b, diag, x);
 }
 template <class T>
 void launch_mg_projection(cudaStream_t s, int n, const double* r,
                           const uint8_t* active, const T* recursive,
                           Reduce red) {
-  k_mg_projection<T><<<reduction_blocks(n), kThreads, 0, s>>>(n, r, active,
+  launch(k_mg_projection<T>, reduction_blocks(n), kThreads, 0, s, n, r, active,
                                                               recursive, red);
 }
 
 void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
                      double* y, Reduce red) {
-  k_spmv_dot<<<reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, y, red);
+  launch(k_spmv_dot, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, x, y, red);
 }
 void launch_residual_norm(cudaStream_t s, const Level<double>& L,
                           const double* x, const double* b, double* r,
                           Reduce red) {
-  k_residual_norm<<<reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s>>>(L, x, b, r,
+  launch(k_residual_norm, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, x, b, r,
                                                                        red);
 }
 void launch_pcg_update(cudaStream_t s, int n, double* x, const double* p,
                        double* r, const double* ap, Reduce red) {
-  k_pcg_update<<<reduction_blocks(n), kThreads, 0, s>>>(n, x, p, r, ap, red);
+  launch(k_pcg_update, reduction_blocks(n), kThreads, 0, s, n, x, p, r, ap, red);
 }
 void launch_dot(cudaStream_t s, int n, const double* a, const double* b,
                 Reduce red) {
-  k_dot<<<reduction_blocks(n), kThreads, 0, s>>>(n, a, b, red);
+  launch(k_dot, reduction_blocks(n), kThreads, 0, s, n, a, b, red);
 }
 void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red) {
-  k_norm2<<<reduction_blocks(n), kThreads, 0, s>>>(n, v, red);
+  launch(k_norm2, reduction_blocks(n), kThreads, 0, s, n, v, red);
 }
 void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc) {
-  k_p_update<<<grid_for(n), kThreads, 0, s>>>(n, p, z, sc);
+  launch(k_p_update, grid_for(n), kThreads, 0, s, n, p, z, sc);
 }
 void launch_copy(cudaStream_t s, int n, const double* src, double* dst) {
-  k_copy<<<grid_for(n), kThreads, 0, s>>>(n, src, dst);
+  launch(k_copy, grid_for(n), kThreads, 0, s, n, src, dst);
 }
 
 void launch_mask_finest(cudaStream_t s, int nx, int ny, int nz,
@@ -1032,29 +1077,27 @@ void launch_mask_finest(cudaStream_t s, int nx, int ny, int nz,
   const long long faces = static_cast<long long>(nx + 1) * ny * nz +
                           static_cast<long long>(nx) * (ny + 1) * nz +
                           static_cast<long long>(nx) * ny * (nz + 1);
-  k_mask_faces<<<grid_for(faces), kThreads, 0, s>>>(nx, ny, nz, fx_in, fy_in, fz_in,
+  launch(k_mask_faces, grid_for(faces), kThreads, 0, s, nx, ny, nz, fx_in, fy_in, fz_in,
                                                     active, fx, fy, fz);
-  k_mask_cells<<<grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s>>>(
+  launch(k_mask_cells, grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s, 
       nx, ny, nz, x_faces, y_faces, z_faces, diag_in, fx_in, fy_in, fz_in, active,
       diag, fx, fy, fz, volume, fluid);
 }
 void launch_reaction(cudaStream_t s, const Level<double>& L,
                      const double* volume, double* reaction) {
-  k_reaction<<<grid_for(HFPS_CELLS(L)), kThreads, 0, s>>>(L, volume, reaction);
+  launch(k_reaction, grid_for(HFPS_CELLS(L)), kThreads, 0, s, L, volume, reaction);
 }
 void launch_aggregate_axis(cudaStream_t s, const double* src, int ex, int ey,
                            int ez, double* dst, int dx, int dy, int dz,
                            int axis, int face_axis, int global_extent) {
-  k_aggregate_axis<<<grid_for(static_cast<long long>(dx) * dy * dz), kThreads, 0,
-                     s>>>(src, ex, ey, ez, dst, dx, dy, dz, axis, face_axis,
+  launch(k_aggregate_axis, grid_for(static_cast<long long>(dx) * dy * dz), kThreads, 0, s, src, ex, ey, ez, dst, dx, dy, dz, axis, face_axis,
                           global_extent);
 }
 void launch_coarse_diagonal(cudaStream_t s, int nx, int ny, int nz,
                             double* diag, const double* fx, const double* fy,
                             const double* fz, const double* volume,
                             uint8_t* fluid) {
-  k_coarse_diagonal<<<grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0,
-                      s>>>(nx, ny, nz, diag, fx, fy, fz, volume, fluid);
+  launch(k_coarse_diagonal, grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s, nx, ny, nz, diag, fx, fy, fz, volume, fluid);
 }
 void launch_beta_coefficients(cudaStream_t s, int nx, int ny, int nz,
                               const double* x_faces, const double* y_faces,
@@ -1065,19 +1108,18 @@ void launch_beta_coefficients(cudaStream_t s, int nx, int ny, int nz,
   const long long faces = static_cast<long long>(nx + 1) * ny * nz +
                           static_cast<long long>(nx) * (ny + 1) * nz +
                           static_cast<long long>(nx) * ny * (nz + 1);
-  k_beta_faces<<<grid_for(faces), kThreads, 0, s>>>(nx, ny, nz, x_faces, y_faces,
+  launch(k_beta_faces, grid_for(faces), kThreads, 0, s, nx, ny, nz, x_faces, y_faces,
                                                     z_faces, neumann, beta, fx, fy,
                                                     fz);
-  k_beta_diagonal<<<grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0,
-                    s>>>(nx, ny, nz, fx, fy, fz, storage, diag);
+  launch(k_beta_diagonal, grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s, nx, ny, nz, fx, fy, fz, storage, diag);
 }
 void launch_shortcut_ratio(cudaStream_t s, const Level<double>& L,
                            Reduce red) {
-  k_shortcut_ratio<<<reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s>>>(L, red);
+  launch(k_shortcut_ratio, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, red);
 }
 template <class TO, class TI>
 void launch_convert(cudaStream_t s, size_t n, const TI* src, TO* dst) {
-  k_convert<TO, TI><<<grid_for(static_cast<long long>(n)), kThreads, 0, s>>>(n, src,
+  launch(k_convert<TO, TI>, grid_for(static_cast<long long>(n)), kThreads, 0, s, n, src,
                                                                            dst);
 }
 void launch_face_gradients(cudaStream_t s, const Level<double>& L,
@@ -1091,11 +1133,11 @@ void launch_face_gradients(cudaStream_t s, const Level<double>& L,
   const long long faces = static_cast<long long>(L.nx + 1) * L.ny * L.nz +
                           static_cast<long long>(L.nx) * (L.ny + 1) * L.nz +
                           static_cast<long long>(L.nx) * L.ny * (L.nz + 1);
-  k_face_gradients<<<grid_for(faces), kThreads, 0, s>>>(L, lambda, p, gx, gy, gz);
+  launch(k_face_gradients, grid_for(faces), kThreads, 0, s, L, lambda, p, gx, gy, gz);
 }
 void launch_adjoint_source(cudaStream_t s, int n, const double* dl_dp,
                            const uint8_t* active, double* out) {
-  k_adjoint_source<<<grid_for(n), kThreads, 0, s>>>(n, dl_dp, active, out);
+  launch(k_adjoint_source, grid_for(n), kThreads, 0, s, n, dl_dp, active, out);
 }
 
 #define HFPS_INSTANTIATE(T)                                                        \

@@ -88,10 +88,18 @@ template <class T>
 void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
                       const T* fac, T* scratch, int axis, int color);
 // Coarsest level in line mode with x/rhs resident in shared memory; returns
-// false when the level is too large for that form.
+// false when the level is too large for that form.  With `columns`, launches
+// 2n blocks that write the columns of the sweeps' affine map x_out = P x_in
+// + M b (P then M, column-major) to x, n = cells of the level.
 template <class T, class TC>
 bool launch_coarse_line(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
-                        const TC* fac, int sweeps, int axis);
+                        const TC* fac, int sweeps, int axis, bool columns = false);
+// out = P x + M b with the dense coarsest-level map built by the columns
+// mode above (n <= kCoarseDenseMaxCells; out must not alias x or b).
+constexpr int kCoarseDenseMaxCells = 2048;
+template <class T>
+void launch_coarse_dense(cudaStream_t s, int n, const double* op, const T* x,
+                         const T* b, T* out);
 
 // Coarsest level: `sweeps` smoother sweeps in one CTA, arithmetic in TC.
 // Line mode when line_axis >= 0 (zebra line Gauss-Seidel).

@@ -268,6 +268,7 @@ struct ScanLayout {
 // Thomas factors of every line, one thread per line, in FP64 whatever T is.
 template <class T>
 __global__ void k_scan_factors(Level<T> L, int axis, T* __restrict__ fac) {
+  grid_dependency_sync();
   const int a_extent = axis == 0 ? L.ny : L.nx;
   const int b_extent = axis == 2 ? L.ny : L.nz;
   const int lines = a_extent * b_extent;
@@ -308,6 +309,7 @@ template <class T, int AXIS, int LPB>
 __global__ void __launch_bounds__(ScanConfig<T>::threads)
     k_line_scan_color(Level<T> L, T* x, const T* __restrict__ rhs,
                       const T* __restrict__ fac, int color, int m) {
+  grid_dependency_sync();
   extern __shared__ unsigned char scan_smem[];
   const int S = blockDim.y;
   T* fA = reinterpret_cast<T*>(scan_smem);
@@ -394,6 +396,7 @@ __global__ void __launch_bounds__(ScanConfig<T>::threads)
 // [2*steps+1][lines][P] so a line's threads read consecutive addresses.
 template <class T>
 __global__ void __launch_bounds__(1024) k_pcr_factors(Level<T> L, int axis, int P, T* __restrict__ fac) {
+  grid_dependency_sync();
   extern __shared__ unsigned char pcr_factor_smem[];
   T* sa = reinterpret_cast<T*>(pcr_factor_smem) + threadIdx.y * 3 * P;
   T* sb = sa + P;
@@ -503,6 +506,7 @@ __global__ void __launch_bounds__(1024) k_line_pcr_factored_color(Level<T> L, T*
                                           const T* __restrict__ rhs,
                                           const T* __restrict__ fac, int axis,
                                           int color) {
+  grid_dependency_sync();
   constexpr int P = 1 << STEPS;
   extern __shared__ unsigned char pcr_rhs_smem[];
   T* sd = reinterpret_cast<T*>(pcr_rhs_smem) + threadIdx.y * P;
@@ -553,10 +557,17 @@ __device__ __forceinline__ void coarse_line_pass(const Level<TC>& L, TC* xs,
 // Coarsest level, line mode: all sweeps in one CTA with x and rhs resident
 // in shared memory (widened to TC).  When each colour's lines fit the CTA's
 // thread rows, both colours' PCR factors stay in registers for all sweeps.
+//
+// With `columns` set, block j instead starts from unit data, x = e_j and
+// b = 0 for j < n, x = 0 and b = e_{j-n} for j >= n, and writes its result
+// to x + j*n: the columns of the affine map x_out = P x_in + M b that the
+// sweeps apply (coarse_dense_operator).
 template <class T, class TC, int STEPS>
 __global__ void __launch_bounds__(512)
     k_coarse_line_smem(Level<TC> L, T* __restrict__ x, const T* __restrict__ b,
-                       const TC* __restrict__ fac, int sweeps, int axis) {
+                       const TC* __restrict__ fac, int sweeps, int axis,
+                       bool columns) {
+  grid_dependency_sync();
   constexpr int P = 1 << STEPS;
   extern __shared__ unsigned char coarse_smem[];
   const int n = L.nx * L.ny * L.nz;
@@ -565,9 +576,18 @@ __global__ void __launch_bounds__(512)
   TC* sd = bs + n + threadIdx.y * P;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   const int nthreads = blockDim.x * blockDim.y;
-  for (int c = tid; c < n; c += nthreads) {
-    xs[c] = static_cast<TC>(x[c]);
-    bs[c] = static_cast<TC>(b[c]);
+  if (columns) {
+    const int j = blockIdx.x;
+    for (int c = tid; c < n; c += nthreads) {
+      xs[c] = (j < n && c == j) ? TC(1) : TC(0);
+      bs[c] = (j >= n && c == j - n) ? TC(1) : TC(0);
+    }
+    x += static_cast<size_t>(j) * n;
+  } else {
+    for (int c = tid; c < n; c += nthreads) {
+      xs[c] = static_cast<TC>(x[c]);
+      bs[c] = static_cast<TC>(b[c]);
+    }
   }
   __syncthreads();
   const int extent = line_extent(axis, L.nx, L.ny, L.nz);
@@ -654,7 +674,7 @@ void launch_scan(cudaStream_t s, const Level<T>& L, T* x, const T* b, const T* f
                  int color, long long per_color, const ScanShape& sh) {
   const int blocks = static_cast<int>((per_color + LPB - 1) / LPB);
   const size_t smem = static_cast<size_t>(4) * sh.chunks * LPB * sizeof(T);
-  k_line_scan_color<T, AXIS, LPB><<<blocks, dim3(LPB, sh.chunks), smem, s>>>(L, x, b, fac, color,
+  launch(k_line_scan_color<T, AXIS, LPB>, blocks, dim3(LPB, sh.chunks), smem, s, L, x, b, fac, color,
                                                                              sh.rows);
 }
 
@@ -704,13 +724,13 @@ void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac) {
   const int kind = line_kind(L.nx, L.ny, L.nz, axis);
   if (kind == kLineNone) return;
   if (kind == kLineScan) {
-    k_scan_factors<T><<<(lines + 127) / 128, 128, 0, s>>>(L, axis, fac);
+    launch(k_scan_factors<T>, (lines + 127) / 128, 128, 0, s, L, axis, fac);
     return;
   }
   int P, lpb, steps;
   pcr_shape(extent, P, lpb, steps);
   const size_t smem = static_cast<size_t>(3) * P * lpb * sizeof(T);
-  k_pcr_factors<T><<<(lines + lpb - 1) / lpb, dim3(P, lpb), smem, s>>>(L, axis, P, fac);
+  launch(k_pcr_factors<T>, (lines + lpb - 1) / lpb, dim3(P, lpb), smem, s, L, axis, P, fac);
 }
 
 template <class T>
@@ -738,7 +758,7 @@ void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
   switch (steps) {
 #define HFPS_PCR_CASE(N)                                                        \
   case N:                                                                       \
-    k_line_pcr_factored_color<T, N><<<blocks, block, smem, s>>>(L, x, b, fac, axis, \
+    launch(k_line_pcr_factored_color<T, N>, blocks, block, smem, s, L, x, b, fac, axis, \
                                                                  color);        \
     break;
     HFPS_PCR_CASE(0) HFPS_PCR_CASE(1) HFPS_PCR_CASE(2) HFPS_PCR_CASE(3) HFPS_PCR_CASE(4)
@@ -751,7 +771,7 @@ void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
 
 template <class T, class TC>
 bool launch_coarse_line(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
-                        const TC* fac, int sweeps, int axis) {
+                        const TC* fac, int sweeps, int axis, bool columns) {
   const int extent = line_extent(axis, L.nx, L.ny, L.nz);
   if (line_kind(L.nx, L.ny, L.nz, axis) != kLinePcr) return false;
   int P, lpb, steps;
@@ -771,7 +791,8 @@ bool launch_coarse_line(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
       cudaFuncSetAttribute(k_coarse_line_smem<T, TC, N>,                         \
                            cudaFuncAttributeMaxDynamicSharedMemorySize,          \
                            static_cast<int>(smem));                              \
-    k_coarse_line_smem<T, TC, N><<<1, block, smem, s>>>(L, x, b, fac, sweeps, axis); \
+    launch(k_coarse_line_smem<T, TC, N>, columns ? 2 * static_cast<int>(cells) : 1, block, smem, \
+                                    s, L, x, b, fac, sweeps, axis, columns);       \
     break;
     HFPS_COARSE_CASE(0) HFPS_COARSE_CASE(1) HFPS_COARSE_CASE(2) HFPS_COARSE_CASE(3)
     HFPS_COARSE_CASE(4) HFPS_COARSE_CASE(5) HFPS_COARSE_CASE(6) HFPS_COARSE_CASE(7)
@@ -789,8 +810,70 @@ template void launch_line_pass<double>(cudaStream_t, const Level<double>&, doubl
 template void launch_line_pass<float>(cudaStream_t, const Level<float>&, float*, const float*,
                                       const float*, float*, int, int);
 template bool launch_coarse_line<double, double>(cudaStream_t, const Level<double>&, double*,
-                                                 const double*, const double*, int, int);
+                                                 const double*, const double*, int, int, bool);
 template bool launch_coarse_line<float, double>(cudaStream_t, const Level<double>&, float*,
-                                                const float*, const double*, int, int);
+                                                const float*, const double*, int, int, bool);
+
+// ---------------------------------------------------------------------------
+// Coarsest level as a dense affine map: out = P x + M b, with P and M
+// (n x n each, FP64) stored column-major one after the other, as the
+// columns mode of k_coarse_line_smem writes them.  A block owns 32 rows (one
+// per lane); its 32 warps take every 32nd column with 8 column loads in
+// flight per thread, and the 32 partial sums of a row are added in warp
+// order, so the result is reproducible.
+constexpr int kDenseWarps = 32;
+constexpr int kDenseUnroll = 8;
+
+template <class T>
+__global__ void __launch_bounds__(32 * kDenseWarps)
+    k_coarse_dense(int n, const double* __restrict__ op, const T* __restrict__ x,
+                   const T* __restrict__ b, T* __restrict__ out) {
+  grid_dependency_sync();
+  extern __shared__ double dense_smem[];
+  double* v = dense_smem;                    // [2n]: x then b, widened
+  double* part = dense_smem + 2 * n;         // [kDenseWarps][32]
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  for (int j = tid; j < n; j += 32 * kDenseWarps) {
+    v[j] = static_cast<double>(x[j]);
+    v[n + j] = static_cast<double>(b[j]);
+  }
+  __syncthreads();
+  const int row = min(blockIdx.x * 32 + threadIdx.x, n - 1);
+  const int cols = 2 * n;
+  double acc = 0.0;
+  for (int j0 = threadIdx.y; j0 < cols; j0 += kDenseWarps * kDenseUnroll) {
+    double m[kDenseUnroll];
+#pragma unroll
+    for (int u = 0; u < kDenseUnroll; ++u) {
+      const int j = min(j0 + u * kDenseWarps, cols - 1);
+      m[u] = __ldg(op + static_cast<size_t>(j) * n + row);
+    }
+#pragma unroll
+    for (int u = 0; u < kDenseUnroll; ++u)
+      if (j0 + u * kDenseWarps < cols) acc += m[u] * v[j0 + u * kDenseWarps];
+  }
+  part[threadIdx.y * 32 + threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.y == 0 && blockIdx.x * 32 + threadIdx.x < n) {
+    double sum = part[threadIdx.x];
+    for (int w = 1; w < kDenseWarps; ++w) sum += part[w * 32 + threadIdx.x];
+    out[blockIdx.x * 32 + threadIdx.x] = static_cast<T>(sum);
+  }
+}
+
+template <class T>
+void launch_coarse_dense(cudaStream_t s, int n, const double* op, const T* x,
+                         const T* b, T* out) {
+  const size_t smem = (2 * static_cast<size_t>(n) + 32 * kDenseWarps) * sizeof(double);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_coarse_dense<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+  launch(k_coarse_dense<T>, (n + 31) / 32, dim3(32, kDenseWarps), smem, s, n, op, x, b, out);
+}
+
+template void launch_coarse_dense<double>(cudaStream_t, int, const double*, const double*,
+                                          const double*, double*);
+template void launch_coarse_dense<float>(cudaStream_t, int, const double*, const float*,
+                                         const float*, float*);
 
 }  // namespace hfps

@@ -264,6 +264,19 @@ Status Solver::allocate() {
   for (auto& k : k_off) k = add(cells * 8);
   const size_t scalars_off = add(sizeof(Scalars));
   const size_t partials_off = add(sizeof(double) * 3 * 148 * 8 + 4096);
+  // Dense affine map of the coarsest-level sweeps (one line axis, few cells).
+  const Shape& last = shapes.back();
+  const int last_cells = last.n[0] * last.n[1] * last.n[2];
+  size_t dense_off = SIZE_MAX;
+  coarse_axis_ = -1;
+  if (last.line_mask != 0 && (last.line_mask & (last.line_mask - 1)) == 0 &&
+      last_cells <= kCoarseDenseMaxCells) {
+    const int axis = last.line_mask == 1 ? 0 : (last.line_mask == 2 ? 1 : 2);
+    if (line_kind(last.n[0], last.n[1], last.n[2], axis) == kLinePcr) {
+      coarse_axis_ = axis;
+      dense_off = add(2 * static_cast<size_t>(last_cells) * last_cells * 8);
+    }
+  }
   arena_bytes_ = bytes;
   Status st = check(cudaMalloc(&arena_, arena_bytes_), "device arena");
   if (!st) return st;
@@ -298,6 +311,7 @@ Status Solver::allocate() {
   kb_ = reinterpret_cast<double*>(at(k_off[5]));
   d_scalars_ = reinterpret_cast<Scalars*>(at(scalars_off));
   d_partials_ = reinterpret_cast<double*>(at(partials_off));
+  coarse_op_ = dense_off == SIZE_MAX ? nullptr : reinterpret_cast<double*>(at(dense_off));
   l64_.resize(levels);
   l32_.resize(levels);
   volume_.resize(levels);
@@ -414,6 +428,15 @@ Status Solver::build_hierarchy() {
   for (auto& L : l64_)
     for (int a = 0; a < 3; ++a)
       if (L.lfac[a] != nullptr) launch_line_factors<double>(stream_, L.view(neumann_), a, L.lfac[a]);
+  // The coarsest level's sweeps (from any x_in and b) are one affine map;
+  // record its columns once per coefficient update.
+  coarse_dense_ = false;
+  if (coarse_op_ != nullptr) {
+    const DeviceLevel<double>& D = l64_.back();
+    coarse_dense_ = launch_coarse_line<double, double>(
+        stream_, D.view(neumann_), coarse_op_, nullptr, D.lfac[coarse_axis_],
+        policy_.coarse_sweeps, coarse_axis_, true);
+  }
   Status st = check(cudaGetLastError(), "hierarchy kernels");
   if (!st) return st;
   // Diagonal shortcut (select_diagonal_shortcut, src/solver_mg.cpp:1577-1611).
@@ -590,6 +613,11 @@ void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels) {
   if (L.line_mask == 0) {
     launch_coarse_solve<T, double>(stream_, view, L.x, L.b, xs, bs, D.t, D.r,
                                    policy_.coarse_sweeps, -1);
+    return;
+  }
+  if (coarse_dense_) {
+    launch_coarse_dense<T>(stream_, L.cells(), coarse_op_, L.x, L.b, L.t);
+    std::swap(L.x, L.t);
     return;
   }
   for (int a = 0; a < 3; ++a) {

@@ -139,6 +139,14 @@ class Solver {
   bool coefficients_ready_{};
   bool mixed_ready_{};
   bool diagonal_shortcut_{};
+  // Coarsest level in line mode with one line axis and at most
+  // kCoarseDenseMaxCells cells: its coarse_sweeps zebra line sweeps are an
+  // affine map x_out = P x_in + M b, recorded column by column after every
+  // coefficient update and applied as one dense product (P then M, FP64,
+  // column-major).
+  double* coarse_op_{};
+  int coarse_axis_{-1};
+  bool coarse_dense_{};
   cudaGraphExec_t mg_graph_[2]{};
   size_t mg_nodes_[2]{};      // kernels per MG application (graph nodes)
   uint64_t launches_{};       // kernels launched since the last reset
