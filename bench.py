@@ -275,6 +275,11 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes per level-0 cell of one zebra colour pass of the FP64 line
+# kernel, from one ncu capture at 256x256x128 (377.8 MB read + 48.2 MB
+# written over 8,388,608 cells); traffic grows with the cell count.
+LINE_PASS_DRAM_BYTES_PER_CELL = (377.820672e6 + 48.243456e6) / (256 * 256 * 128)
+
 # Iterations the reference solve_pcg (production MG, unit_linear) needs per
 # warm-started solve of this workload: 41, 41, 41 for steps 1-3, measured by
 # running the compiled reference to convergence on the same inputs (the cold
@@ -381,7 +386,10 @@ def run_b200(args, world, rank, local):
                 "kernel": "k_line_scan_color<double,y,8> level 0 (one zebra colour)",
                 "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": dom["gbs"] / peak, "peak_source": peak_note,
-                "traffic": None, "bytes_per_launch": dom["bytes"], "ms_per_launch": dom["ms"]}
+                "traffic": LINE_PASS_DRAM_BYTES_PER_CELL * n,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at "
+                                  "256x256x128, scaled by cells",
+                "bytes_per_launch": dom["bytes"], "ms_per_launch": dom["ms"]}
 
     iterations = [i["iterations"] for i in infos]
     cpu = None
