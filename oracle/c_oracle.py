@@ -44,6 +44,9 @@ def _load():
         lib.hfo_apply_mg.argtypes = [ctypes.c_void_p, dp, dp]
         lib.hfo_solve.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int]
+        lib.hfo_solve_fgmres.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, dp, dp, ctypes.c_int]
         _lib = lib
     return _lib
 
@@ -134,13 +137,21 @@ class OracleSession:
         return z
 
     def solve(self, rhs, x0: Optional[np.ndarray] = None, rtol=1e-10, atol=0.0, maxit=400,
-              true_residual_interval=4):
+              true_residual_interval=4, algorithm: str = "pcg", restart: int = 12):
+        """solve_pcg, or solve_fgmres(restart) when ``algorithm == "fgmres"``
+        (build the session with unit_linear=False for the reference's
+        residual-minimising MG scaling)."""
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         x = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64, order="C")
         out = np.zeros(8)
         hist = np.zeros(maxit)
-        rc = self._lib.hfo_solve(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
-                                 true_residual_interval, _dp(out), _dp(hist), maxit)
+        if algorithm == "fgmres":
+            rc = self._lib.hfo_solve_fgmres(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
+                                            true_residual_interval, restart, _dp(out), _dp(hist),
+                                            maxit)
+        else:
+            rc = self._lib.hfo_solve(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
+                                     true_residual_interval, _dp(out), _dp(hist), maxit)
         it = int(out[0])
         info = {
             "status": rc,

@@ -875,6 +875,242 @@ done:
 }
 
 /* ------------------------------------------------------------------ */
+/* solve_fgmres (src/solver_krylov.cpp:1557-2650): single-reduction      */
+/* Arnoldi on the shifted image w = A z - v (shift 1, :35), one batched */
+/* reduction for the projections and |w|^2 (local_multidot, :206-244),  */
+/* the Pythagorean norm with its breakdown fallbacks                     */
+/* (single_reduction_fgmres_norm, :565-609), Givens rotations, true-     */
+/* residual audits of the candidate every true_residual_interval         */
+/* iterations and at cycle ends, restarts.  Subspace recycling and the   */
+/* convergence audit are inactive, as in the reference harness.          */
+/* ------------------------------------------------------------------ */
+#define FGMRES_SHIFT 1.0
+
+/* add_scaled_basis (:510-564): dst = dst + s_0 b_0 + s_1 b_1 + ... per cell. */
+static int add_scaled_basis(double* dst, double* const* src, const double* s,
+                            int count, size_t n) {
+  int ok = 1;
+  for (size_t c = 0; c < n; ++c) {
+    double v = dst[c];
+    for (int r = 0; r < count; ++r) v = v + s[r] * src[r][c];
+    if (!isfinite(v)) ok = 0;
+    dst[c] = v;
+  }
+  return ok;
+}
+
+static int back_substitute(const double* h, const double* g, double* y, int count,
+                           int rows) {
+  for (int row = count - 1; row >= 0; --row) {
+    double value = g[row];
+    for (int upper = row + 1; upper < count; ++upper)
+      value -= h[(size_t)upper * rows + row] * y[upper];
+    const double divisor = h[(size_t)row * rows + row];
+    if (divisor == 0.0 || !isfinite(divisor)) return TERM_BREAKDOWN;
+    y[row] = value / divisor;
+    if (!isfinite(y[row])) return TERM_NON_FINITE;
+  }
+  return -1;
+}
+
+int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
+                     double atol, int maxit, int tri, int restart, double* out,
+                     double* history, int hcap) {
+  oracle_t* o = handle;
+  const size_t n = o->lv[0].cells;
+  int ok = 1;
+  long op_applies = 0, pc_applies = 0;
+  int it = 0;
+  int term = TERM_MAXIMUM, status = 6;
+  memset(out, 0, 8 * sizeof(double));
+  if (restart < 1 || restart > 64) { out[3] = TERM_BREAKDOWN; return 2; }
+  const int rows = restart + 1;
+  double** V = calloc((size_t)rows, sizeof(double*));
+  double** Z = calloc((size_t)restart, sizeof(double*));
+  double* ax = malloc(n * sizeof(double));
+  double* h = calloc((size_t)rows * restart, sizeof(double));
+  double* cs = calloc((size_t)restart, sizeof(double));
+  double* sn = calloc((size_t)restart, sizeof(double));
+  double* g = calloc((size_t)rows, sizeof(double));
+  double* y = calloc((size_t)restart, sizeof(double));
+  double* scratch = calloc((size_t)rows + 1, sizeof(double));
+  double* scales = calloc((size_t)rows, sizeof(double));
+  for (int i = 0; i < rows; ++i) V[i] = malloc(n * sizeof(double));
+  for (int i = 0; i < restart; ++i) Z[i] = malloc(n * sizeof(double));
+
+  const double bnorm = norm2(rhs, n, &ok);
+  double initial = 0.0, final_true = 0.0, recursive = 0.0;
+  if (!ok) { term = TERM_NON_FINITE; status = 5; goto done; }
+  const double tol = atol > rtol * bnorm ? atol : rtol * bnorm;
+  out[4] = bnorm;
+  out[5] = tol;
+  if (bnorm == 0.0) {
+    memset(x, 0, n * sizeof(double));
+    term = TERM_ZERO_RHS; status = 0; goto done;
+  }
+  /* compute_true_residual (:1071-1092): v0 = 1.0 b + -1.0 A x, |v0|. */
+#define TRUE_RESIDUAL(dst_norm, sol)                                       \
+  do {                                                                     \
+    hfo_apply_operator(o, sol, ax);                                        \
+    ++op_applies;                                                          \
+    for (size_t c = 0; c < n; ++c) V[0][c] = 1.0 * rhs[c] + -1.0 * ax[c];  \
+    dst_norm = norm2(V[0], n, &ok);                                        \
+  } while (0)
+  TRUE_RESIDUAL(initial, x);
+  final_true = initial;
+  recursive = initial;
+  if (!ok) { term = TERM_NON_FINITE; status = 5; goto done; }
+  if (initial <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+  int deferred = 0;
+  while (it < maxit) {
+    const double beta = final_true;
+    const double inv_beta = 1.0 / beta;
+    for (size_t c = 0; c < n; ++c) V[0][c] = inv_beta * V[0][c];
+    for (int i = 0; i < rows; ++i) g[i] = 0.0;
+    g[0] = beta;
+    int restarted = 0;
+    for (int column = 0; column < restart && it < maxit; ++column) {
+      double* v = V[column];
+      hfo_apply_mg(o, v, Z[column]);
+      ++pc_applies;
+      hfo_apply_operator(o, Z[column], ax);
+      ++op_applies;
+      for (size_t c = 0; c < n; ++c) ax[c] = ax[c] + -FGMRES_SHIFT * v[c];
+      const int count = column + 1;
+      /* local_multidot: Neumaier dots v_i . w and w . w */
+      double* column_h = h + (size_t)column * rows;
+      for (int i = 0; i <= count; ++i) {
+        const double* left = i == count ? ax : V[i];
+        column_h[i] = dot(left, ax, n, &ok);
+      }
+      if (!ok) { term = TERM_NON_FINITE; status = 5; goto done; }
+      const double bar_norm = column_h[count];
+      for (int r = 0; r < count; ++r) scales[r] = -column_h[r];
+      /* single_reduction_fgmres_norm */
+      double t = bar_norm;
+      for (int r = 0; r < count; ++r) t = t - column_h[r] * column_h[r];
+      int unsafe = 0;
+      double next_norm;
+      if (!isfinite(t)) { term = TERM_NON_FINITE; status = 5; goto done; }
+      if (t < 0.0) { unsafe = 1; next_norm = 0.0; }
+      else next_norm = sqrt(t);
+      if (unsafe && column != 0) {
+        /* Discard the column: finish the cycle on the previous columns. */
+        ++it;
+        const int valid = column;
+        const int bs = back_substitute(h, g, y, valid, rows);
+        if (bs >= 0) { term = bs; status = 5; goto done; }
+        if (!add_scaled_basis(x, Z, y, valid, n)) { term = TERM_NON_FINITE; status = 5; goto done; }
+        TRUE_RESIDUAL(final_true, x);
+        recursive = final_true;
+        if (history && it - 1 < hcap) history[it - 1] = recursive;
+        if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+        if (it == maxit) { term = TERM_MAXIMUM; status = 6; goto done; }
+        memset(h, 0, (size_t)rows * restart * sizeof(double));
+        memset(cs, 0, (size_t)restart * sizeof(double));
+        memset(sn, 0, (size_t)restart * sizeof(double));
+        memset(g, 0, (size_t)rows * sizeof(double));
+        memset(y, 0, (size_t)restart * sizeof(double));
+        restarted = 1;
+        break;
+      }
+      int explicit_orth = 0;
+      if (unsafe || next_norm == 0.0) {
+        /* Explicit second orthogonalisation pass, measured stably. */
+        add_scaled_basis(ax, V, scales, count, n);
+        for (int r = 0; r < count; ++r) y[r] = dot(V[r], ax, n, &ok);
+        for (int r = 0; r < count; ++r) {
+          column_h[r] += y[r];
+          scales[r] = -y[r];
+        }
+        add_scaled_basis(ax, V, scales, count, n);
+        next_norm = norm2(ax, n, &ok);
+        if (!ok) { term = TERM_NON_FINITE; status = 5; goto done; }
+        explicit_orth = 1;
+      }
+      column_h[column] += FGMRES_SHIFT;
+      column_h[column + 1] = next_norm;
+      for (int r = 0; r < column; ++r) {
+        double* upper = &h[(size_t)column * rows + r];
+        double* lower = &h[(size_t)column * rows + r + 1];
+        const double rotated = cs[r] * *upper + sn[r] * *lower;
+        *lower = -sn[r] * *upper + cs[r] * *lower;
+        *upper = rotated;
+      }
+      double* diagonal = &h[(size_t)column * rows + column];
+      double* subdiagonal = &h[(size_t)column * rows + column + 1];
+      const double rotation_norm = hypot(*diagonal, *subdiagonal);
+      if (!(rotation_norm > 0.0) || !isfinite(rotation_norm)) {
+        term = TERM_BREAKDOWN; status = 5; goto done;
+      }
+      cs[column] = *diagonal / rotation_norm;
+      sn[column] = *subdiagonal / rotation_norm;
+      *diagonal = rotation_norm;
+      *subdiagonal = 0.0;
+      g[column + 1] = -sn[column] * g[column];
+      g[column] = cs[column] * g[column];
+      recursive = fabs(g[column + 1]);
+      ++it;
+      if (history && it - 1 < hcap) history[it - 1] = recursive;
+      const int happy = next_norm == 0.0;
+      const int cycle_end = happy || column + 1 == restart || it == maxit;
+      const int verify = happy || (!deferred && recursive <= tol) || it % tri == 0 ||
+                         cycle_end;
+      if (!cycle_end) {
+        if (!explicit_orth) add_scaled_basis(ax, V, scales, count, n);
+        const double inv = 1.0 / next_norm;
+        for (size_t c = 0; c < n; ++c) V[column + 1][c] = inv * ax[c];
+      }
+      if (!verify) continue;
+      const int bs = back_substitute(h, g, y, count, rows);
+      if (bs >= 0) { term = bs; status = 5; goto done; }
+      if (!cycle_end) {
+        /* Audit the candidate in the unused last basis slot. */
+        double* trial = V[restart];
+        memcpy(trial, x, n * sizeof(double));
+        add_scaled_basis(trial, Z, y, count, n);
+        hfo_apply_operator(o, trial, ax);
+        ++op_applies;
+        for (size_t c = 0; c < n; ++c) ax[c] = 1.0 * rhs[c] + -1.0 * ax[c];
+        const double audited = norm2(ax, n, &ok);
+        final_true = audited;
+        if (audited <= tol) {
+          memcpy(x, trial, n * sizeof(double));
+          term = TERM_CONVERGED; status = 0; goto done;
+        }
+        continue;
+      }
+      add_scaled_basis(x, Z, y, count, n);
+      TRUE_RESIDUAL(final_true, x);
+      recursive = final_true;
+      if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+      if (it == maxit) { term = TERM_MAXIMUM; status = 6; goto done; }
+      if (happy) {
+        const double guard = 64.0 * DBL_EPSILON * (beta > tol ? beta : tol);
+        if (!(final_true + guard < beta)) { term = TERM_BREAKDOWN; status = 5; goto done; }
+      }
+      restarted = 1;
+      break;
+    }
+    if (!restarted) break;
+  }
+done:
+#undef TRUE_RESIDUAL
+  out[0] = it;
+  out[1] = initial;
+  out[2] = final_true;
+  out[3] = term;
+  out[6] = (double)op_applies;
+  out[7] = (double)pc_applies;
+  for (int i = 0; i < rows; ++i) free(V[i]);
+  for (int i = 0; i < restart; ++i) free(Z[i]);
+  free(V); free(Z); free(ax); free(h); free(cs); free(sn); free(g); free(y);
+  free(scratch); free(scales);
+  (void)recursive;
+  return ok ? status : 5;
+}
+
+/* ------------------------------------------------------------------ */
 void* hfo_create(int nx, int ny, int nz, const double* xf, const double* yf,
                  const double* zf, const int* bc, const double* diagonal,
                  const double* fx, const double* fy, const double* fz,

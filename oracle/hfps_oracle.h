@@ -47,6 +47,14 @@ int hfo_solve(void* handle, const double* rhs, double* x,
               int maximum_iterations, int true_residual_interval,
               double* outputs, double* history, int history_capacity);
 
+/* solve_fgmres (src/solver_krylov.cpp:1557-2650) with the MG plan as the
+ * (flexible) preconditioner; same outputs and history as hfo_solve. */
+int hfo_solve_fgmres(void* handle, const double* rhs, double* x,
+                     double relative_tolerance, double absolute_tolerance,
+                     int maximum_iterations, int true_residual_interval,
+                     int restart, double* outputs, double* history,
+                     int history_capacity);
+
 #ifdef __cplusplus
 }
 #endif

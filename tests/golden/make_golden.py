@@ -6,9 +6,10 @@ Run in a tree where the reference sources are present:
 
 For each small case the script builds the seeded system with
 hfps.workloads, then records what the reference's own code returns for it
-(oracle/_ref: NativeCartesianMgPlan::apply, the IBM-decorated operator and
-solve_pcg with the MG plan): the MG correction of a seeded vector, the
-operator action, and the solution/iteration count at rtol 1e-13.  A checksum
+(oracle/_ref: NativeCartesianMgPlan::apply, the IBM-decorated operator,
+solve_pcg with the unit-scaled MG plan and solve_fgmres(12) with the
+residual-minimising one): the MG correction of a seeded vector, the operator
+action, and the solutions/iteration counts at rtol 1e-13.  A checksum
 of the inputs pins the generator, so a changed generator fails the tests
 instead of silently comparing different systems.
 """
@@ -74,15 +75,24 @@ def main():
         op = ref.apply_operator(v)
         x, info = ref.solve(system.rhs, rtol=1e-13, maxit=400)
         x10, info10 = ref.solve(system.rhs, rtol=1e-10, maxit=400)
-        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), mg=mg, op=op, x=x, x10=x10)
+        levels = ref.levels()
+        ref.close()
+        fg = ref_oracle.RefSession(system, policy, algorithm="fgmres", restart=12)
+        mg_rm = fg.apply_mg(v)
+        xf, infof = fg.solve(system.rhs, rtol=1e-13, maxit=400)
+        fg.close()
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), mg=mg, op=op, x=x, x10=x10,
+                            mg_residual_minimising=mg_rm, x_fgmres=xf)
         index[name] = {
             "spec": spec, "policy": pol, "digest": input_digest(system),
-            "levels": ref.levels(),
+            "levels": levels,
             "iterations_1e13": info["iterations"], "iterations_1e10": info10["iterations"],
             "final_true_residual_1e13": info["final_true_residual"],
             "rhs_norm": info["rhs_norm"],
+            "fgmres_iterations_1e13": infof["iterations"],
+            "fgmres_final_true_residual_1e13": infof["final_true_residual"],
+            "fgmres_operator_applies": infof["operator_applies"],
         }
-        ref.close()
         print(name, index[name]["iterations_1e13"], index[name]["iterations_1e10"])
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(index, f, indent=1)

@@ -2,8 +2,9 @@
 
 The C restatement (oracle/hfps_oracle.c) is pinned three ways:
 * against golden fixtures recorded from the compiled reference sources
-  (tests/golden/make_golden.py): operator action, MG correction and the
-  solve_pcg solution must match bit for bit;
+  (tests/golden/make_golden.py): operator action, MG correction (unit and
+  residual-minimising scaling), the solve_pcg solution and the
+  solve_fgmres(12) solution must match bit for bit;
 * against the compiled reference live, when oracle/_ref is present;
 * against the reference's own known-answer and property tests, ported:
   Chebyshev degrees 1-4 (tests/unit/solver_mg_chebyshev_test.cpp:797-841),
@@ -48,6 +49,42 @@ def test_restatement_reproduces_reference_golden(name):
     assert info["termination"] == "converged"
     assert info["iterations"] == meta["iterations_1e13"]
     assert np.array_equal(x, g["x"])
+
+
+@pytest.mark.parametrize("name", sorted(golden_cases.index()))
+def test_fgmres_restatement_reproduces_reference_golden(name):
+    """solve_fgmres(12) with the residual-minimising MG plan
+    (src/solver_krylov.cpp:1557-2650): same iterations, operator applies and
+    solution bits as the reference."""
+    s = golden_cases.system(name)
+    g = golden_cases.arrays(name)
+    meta = golden_cases.index()[name]
+    o = _oracle(s, golden_cases.policy(name), unit_linear=False)
+    assert np.array_equal(o.apply_mg(golden_cases.probe(s)), g["mg_residual_minimising"])
+    x, info = o.solve(s.rhs, rtol=1e-13, maxit=400, algorithm="fgmres", restart=12)
+    assert info["termination"] == "converged"
+    assert info["iterations"] == meta["fgmres_iterations_1e13"]
+    assert info["operator_applies"] == meta["fgmres_operator_applies"]
+    assert info["final_true_residual"] == meta["fgmres_final_true_residual_1e13"]
+    assert np.array_equal(x, g["x_fgmres"])
+
+
+def test_fgmres_short_restart_matches_live_reference():
+    """Restart lengths below the iteration count exercise the cycle-end
+    restart and the interior true-residual audits."""
+    import ref_oracle
+    if not ref_oracle.available():
+        pytest.skip("compiled reference not built (make -C oracle ref)")
+    s = workloads.make("sphere64", n=(18, 14, 12), seed=8)
+    for restart, tri in ((3, 4), (5, 2), (12, 4)):
+        pol = ref_oracle.MgPolicy.production()
+        r = ref_oracle.RefSession(s, pol, algorithm="fgmres", restart=restart)
+        o = _oracle(s, pol, unit_linear=False)
+        x1, i1 = r.solve(s.rhs, rtol=1e-12, true_residual_interval=tri)
+        x2, i2 = o.solve(s.rhs, rtol=1e-12, true_residual_interval=tri, algorithm="fgmres",
+                         restart=restart)
+        assert (i1["iterations"], i1["operator_applies"]) == (i2["iterations"], i2["operator_applies"])
+        assert np.array_equal(x1, x2)
 
 
 def test_restatement_matches_live_reference():
