@@ -550,6 +550,71 @@ __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
     apply_scalar_op(red.scalars, red.op, v[0]);
 }
 
+// ---------------------------------------------------------------------------
+// FGMRES kernels (solve_fgmres, src/solver_krylov.cpp:1557-2650).
+
+// w = A z + (-shift) v: the operator image of the preconditioned basis
+// vector shifted by the basis vector itself (add_scaled(ax, -shift, v),
+// :2168-2172), in one pass.
+__global__ void k_operator_shift(Level<double> L, const double* __restrict__ z,
+                                 const double* __restrict__ v, double shift,
+                                 double* __restrict__ w) {
+  grid_dependency_sync();
+  const int n = L.nx * L.ny * L.nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, L.nx, L.ny, i, j, k);
+    const double a = row_value(L, z, i, j, k, c);
+    w[c] = a + -shift * v[c];
+  }
+}
+
+// Up to kBasisChunk dot products v_r . w (and w . w when `self`), one pass
+// over w; deterministic block partials finished by the last block
+// (local_multidot + checked_sum, :206-244).
+__global__ void k_multidot(int n, BasisRefs basis, const double* __restrict__ w,
+                           int self, double* __restrict__ out, Reduce red) {
+  grid_dependency_sync();
+  double acc[kBasisChunk];
+#pragma unroll
+  for (int r = 0; r < kBasisChunk; ++r) acc[r] = 0.0;
+  const int count = basis.count;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const double wc = w[c];
+#pragma unroll
+    for (int r = 0; r < kBasisChunk; ++r) {
+      if (r < count) acc[r] += __ldg(basis.v[r] + c) * wc;
+      else if (r == count && self) acc[r] += wc * wc;
+    }
+  }
+  if (finish_reduction<kBasisChunk>(acc, red) && threadIdx.x == 0) {
+    for (int r = 0; r < count + (self ? 1 : 0); ++r) out[r] = acc[r];
+    int bad = 0;
+    for (int r = 0; r < count + (self ? 1 : 0); ++r) bad |= !isfinite(acc[r]);
+    if (bad) red.scalars->flags |= 1;
+  }
+}
+
+// out = scale * (dst + s_0 v_0 + s_1 v_1 + ...), terms added per cell in
+// basis order (add_scaled_basis, :510-564), then optionally scaled
+// (scale_copy, :611-625); `out` may be `dst`.
+__global__ void k_basis_update(int n, const double* dst, BasisRefs basis,
+                               double scale, int scaled, double* out) {
+  grid_dependency_sync();
+  const int count = basis.count;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    double v = dst[c];
+#pragma unroll
+    for (int r = 0; r < kBasisChunk; ++r)
+      if (r < count) v = v + basis.s[r] * __ldg(basis.v[r] + c);
+    if (scaled) v = scale * v;
+    out[c] = v;
+  }
+}
+
 __global__ void k_pcg_update(int n, double* __restrict__ x,
                              const double* __restrict__ p,
                              double* __restrict__ r,
@@ -1062,6 +1127,19 @@ void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red) {
 void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc) {
   launch(k_p_update, grid_for(n), kThreads, 0, s, n, p, z, sc);
+}
+void launch_operator_shift(cudaStream_t s, const Level<double>& L, const double* z,
+                           const double* v, double shift, double* w) {
+  launch(k_operator_shift, grid_for(HFPS_CELLS(L)), kThreads, 0, s, L, z, v, shift, w);
+}
+void launch_multidot(cudaStream_t s, int n, const BasisRefs& basis, const double* w,
+                     bool self, double* out, Reduce red) {
+  launch(k_multidot, reduction_blocks(n), kThreads, 0, s, n, basis, w, self ? 1 : 0, out, red);
+}
+void launch_basis_update(cudaStream_t s, int n, const double* dst, const BasisRefs& basis,
+                         double scale, bool scaled, double* out) {
+  launch(k_basis_update, grid_for(n), kThreads, 0, s, n, dst, basis, scale, scaled ? 1 : 0,
+         out);
 }
 void launch_copy(cudaStream_t s, int n, const double* src, double* dst) {
   launch(k_copy, grid_for(n), kThreads, 0, s, n, src, dst);

@@ -26,6 +26,7 @@ struct Scalars {
   double proj[3];    // MG projection sums r.r, r.Az, Az.Az
   double mg_alpha;   // MG correction scale
   double misc[4];
+  double hcol[72];   // FGMRES: projections of the current column and |w|^2
   int flags;         // bit 0 non-finite, bit 1 breakdown
   unsigned counters[8];  // last-block arrival counters, one per reduction
 };
@@ -37,10 +38,15 @@ enum ScalarOp : int {
   kOpRhoRestart = 3, // rho = sum; beta = 0
   kOpMisc = 4,       // misc[0] = sum
 };
+// Arrival counters of reductions that apply no scalar op: 5 MG projection,
+// 6 FGMRES multidot.
+constexpr int kCounterProjection = 5;
+constexpr int kCounterMultidot = 6;
+constexpr int kMaxFgmresRestart = 64;
 
 struct Reduce {
   Scalars* scalars;
-  double* partials;   // >= gridDim.x * 3 doubles
+  double* partials;   // >= gridDim.x * kBasisChunk doubles
   int op;
 };
 
@@ -140,6 +146,24 @@ void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc);
 void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red);
 void launch_copy(cudaStream_t s, int n, const double* src, double* dst);
+// ---- FGMRES (solve_fgmres) ---------------------------------------------------
+// Basis vectors handled by one multidot / basis-update launch.
+constexpr int kBasisChunk = 16;
+struct BasisRefs {
+  const double* v[kBasisChunk];
+  double s[kBasisChunk];
+  int count;
+};
+// w = A z - shift v.
+void launch_operator_shift(cudaStream_t s, const Level<double>& L, const double* z,
+                           const double* v, double shift, double* w);
+// out[r] = v_r . w for r < count, and out[count] = w . w when `self`
+// (count + self <= kBasisChunk); non-finite sums set flags bit 0.
+void launch_multidot(cudaStream_t s, int n, const BasisRefs& basis, const double* w,
+                     bool self, double* out, Reduce red);
+// out = (scaled ? scale : 1) * (dst + sum_r s_r v_r), per cell in basis order.
+void launch_basis_update(cudaStream_t s, int n, const double* dst, const BasisRefs& basis,
+                         double scale, bool scaled, double* out);
 
 // ---- setup (FP64) ---------------------------------------------------------
 void launch_mask_finest(cudaStream_t s, int nx, int ny, int nz,

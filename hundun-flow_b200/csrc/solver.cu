@@ -122,6 +122,7 @@ Solver::~Solver() {
     if (g != nullptr) cudaGraphExecDestroy(g);
   if (h_scalars_ != nullptr) cudaFreeHost(h_scalars_);
   if (arena_ != nullptr) cudaFree(arena_);
+  if (fg_storage_ != nullptr) cudaFree(fg_storage_);
   if (own_stream_ && stream_ != nullptr) cudaStreamDestroy(stream_);
 }
 
@@ -263,7 +264,7 @@ Status Solver::allocate() {
   size_t k_off[6];
   for (auto& k : k_off) k = add(cells * 8);
   const size_t scalars_off = add(sizeof(Scalars));
-  const size_t partials_off = add(sizeof(double) * 3 * 148 * 8 + 4096);
+  const size_t partials_off = add(sizeof(double) * kBasisChunk * 148 * 8 + 4096);
   // Dense affine map of the coarsest-level sweeps (one line axis, few cells).
   const Shape& last = shapes.back();
   const int last_cells = last.n[0] * last.n[1] * last.n[2];
@@ -834,6 +835,330 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
   return fail(HFPS_REJECTED_STEP, kDetailBreakdown, "maximum iterations reached");
 }
 
+Status Solver::ensure_fgmres_storage(uint32_t restart) {
+  if (fg_storage_ != nullptr && restart <= fg_restart_) return {};
+  if (fg_storage_ != nullptr) {
+    Status st = check(cudaStreamSynchronize(stream_), "fgmres storage");
+    if (!st) return st;
+    cudaFree(fg_storage_);
+    fg_storage_ = nullptr;
+  }
+  const size_t n = static_cast<size_t>(nx_) * ny_ * nz_;
+  const size_t stride = (n + 31) & ~static_cast<size_t>(31);
+  const size_t vectors = 2 * static_cast<size_t>(restart) + 2;
+  Status st = check(cudaMalloc(&fg_storage_, vectors * stride * sizeof(double)),
+                    "fgmres basis");
+  if (!st) {
+    fg_storage_ = nullptr;
+    return st;
+  }
+  fg_restart_ = restart;
+  fg_v_.assign(restart + 1, nullptr);
+  fg_z_.assign(restart, nullptr);
+  for (uint32_t i = 0; i <= restart; ++i) fg_v_[i] = fg_storage_ + i * stride;
+  for (uint32_t i = 0; i < restart; ++i) fg_z_[i] = fg_storage_ + (restart + 1 + i) * stride;
+  fg_w_ = fg_storage_ + (2 * static_cast<size_t>(restart) + 1) * stride;
+  return {};
+}
+
+// solve_fgmres (src/solver_krylov.cpp:1557-2650), same control flow: the
+// single-reduction Arnoldi step on w = A z_j - v_j (shift 1, :35) with one
+// batched reduction for the projections and |w|^2, the Pythagorean norm
+// (single_reduction_fgmres_norm, :565-609) with its two fallbacks (discard
+// the column and restart when the recurrence turns unsafe past column 0,
+// explicit re-orthogonalisation at column 0 or a zero norm), Givens
+// rotations, a true-residual audit of the candidate x + Z y in the spare
+// basis slot every true_residual_interval iterations (and at a recursive
+// convergence claim), and a restart from the true residual at cycle ends.
+// Vectors stay on the device; the (restart+1) x restart Hessenberg system,
+// its rotations and back substitution run on the host from one read-back of
+// the column per iteration.
+Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
+                             double* history, uint32_t capacity) {
+  const int n = nx_ * ny_ * nz_;
+  const uint32_t restart = control.restart;
+  const bool mixed = control.precision == HFPS_MIXED;
+  const Level<double> A = l64_[0].view(neumann_);
+  const double kShift = 1.0;
+  const auto red = [&](int op) { return Reduce{d_scalars_, d_partials_, op}; };
+  Status st = ensure_fgmres_storage(restart);
+  if (!st) return st;
+  st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  launch_norm2(stream_, n, kb_, red(kOpMisc));
+  launches_ += 1;
+  st = sync_scalars();
+  if (!st) return st;
+  if (h_scalars_->flags & 1) {
+    result.termination = HFPS_NON_FINITE;
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite rhs");
+  }
+  const double bnorm = std::sqrt(h_scalars_->misc[0]);
+  const double tol = std::max(control.absolute_tolerance,
+                              control.relative_tolerance * bnorm);
+  result.rhs_norm = bnorm;
+  result.true_residual_limit = tol;
+  if (bnorm == 0.0) {
+    st = check(cudaMemsetAsync(kx_, 0, n * sizeof(double), stream_), "zero x");
+    result.termination = HFPS_ZERO_RHS;
+    return st;
+  }
+  std::vector<double*>& V = fg_v_;
+  std::vector<double*>& Z = fg_z_;
+  double* w = fg_w_;
+  // compute_true_residual (:1071-1092): V_0 = b - A x and its norm.
+  const auto true_residual = [&](const double* x, double* r, double& norm) -> Status {
+    launch_residual_norm(stream_, A, x, kb_, r, red(kOpRecursive));
+    launches_ += 1;
+    ++result.operator_applies;
+    Status s = sync_scalars();
+    if (!s) return s;
+    norm = std::sqrt(h_scalars_->rr);
+    if (!std::isfinite(norm)) {
+      result.termination = HFPS_NON_FINITE;
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite residual");
+    }
+    return {};
+  };
+  // dst/out = scale * (dst + sum_r s_r b_r), in chunks of kBasisChunk terms
+  // (the per-cell accumulation order is that of one long loop).
+  const auto basis_update = [&](const double* dst, double* const* b, const double* sc,
+                                int count, double scale, bool scaled, double* out) {
+    int done = 0;
+    do {
+      BasisRefs refs{};
+      refs.count = std::min(kBasisChunk, count - done);
+      for (int r = 0; r < refs.count; ++r) {
+        refs.v[r] = b[done + r];
+        refs.s[r] = sc[done + r];
+      }
+      const bool last = done + refs.count >= count;
+      launch_basis_update(stream_, n, done == 0 ? dst : out, refs, scale, last && scaled, out);
+      launches_ += 1;
+      done += refs.count;
+    } while (done < count);
+  };
+  // hcol[r] = V_r . w (r < count) and hcol[count] = w . w when `self`.
+  const auto multidot = [&](int count, bool self) -> Status {
+    int done = 0;
+    const int total = count + (self ? 1 : 0);
+    do {
+      BasisRefs refs{};
+      refs.count = std::min(kBasisChunk - (self ? 1 : 0), count - done);
+      if (refs.count < 0) refs.count = 0;
+      for (int r = 0; r < refs.count; ++r) refs.v[r] = V[done + r];
+      const bool with_self = self && done + refs.count == count;
+      launch_multidot(stream_, n, refs, w, with_self, d_scalars_->hcol + done,
+                      red(kCounterMultidot));
+      launches_ += 1;
+      done += refs.count + (with_self ? 1 : 0);
+    } while (done < total);
+    Status s = sync_scalars();
+    if (!s) return s;
+    if (h_scalars_->flags & 1) {
+      result.termination = HFPS_NON_FINITE;
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite Arnoldi projection");
+    }
+    return {};
+  };
+
+  double initial = 0.0;
+  st = true_residual(kx_, V[0], initial);
+  if (!st) return st;
+  result.initial_true_residual = initial;
+  result.final_true_residual = initial;
+  result.recursive_residual = initial;
+  if (initial <= tol) {
+    result.termination = HFPS_CONVERGED;
+    return {};
+  }
+  const size_t rows = restart + 1;
+  std::vector<double> h(rows * restart, 0.0), cs(restart, 0.0), sn(restart, 0.0),
+      g(rows, 0.0), y(restart, 0.0), scales(rows, 0.0);
+  uint32_t it = 0;
+  const auto record = [&](double recursive) {
+    result.recursive_residual = recursive;
+    if (history != nullptr && it - 1 < capacity) {
+      history[it - 1] = recursive;
+      result.history_length = it;
+    }
+  };
+  // Back substitution of the rotated Hessenberg system (:2471-2486).
+  const auto solve_y = [&](int count) -> Status {
+    for (int row = count - 1; row >= 0; --row) {
+      double value = g[row];
+      for (int upper = row + 1; upper < count; ++upper)
+        value -= h[static_cast<size_t>(upper) * rows + row] * y[upper];
+      const double divisor = h[static_cast<size_t>(row) * rows + row];
+      if (divisor == 0.0 || !std::isfinite(divisor)) {
+        result.termination = HFPS_BREAKDOWN;
+        return fail(HFPS_NUMERICAL_FAILURE, kDetailBreakdown, "FGMRES breakdown");
+      }
+      y[row] = value / divisor;
+      if (!std::isfinite(y[row])) {
+        result.termination = HFPS_NON_FINITE;
+        return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite FGMRES update");
+      }
+    }
+    return {};
+  };
+  while (it < control.maximum_iterations) {
+    const double beta = result.final_true_residual;
+    basis_update(V[0], nullptr, nullptr, 0, 1.0 / beta, true, V[0]);
+    std::fill(g.begin(), g.end(), 0.0);
+    g[0] = beta;
+    bool restarted = false;
+    for (uint32_t column = 0; column < restart && it < control.maximum_iterations; ++column) {
+      // z_j = M v_j through the MG graph's fixed input/output buffers.
+      launch_copy(stream_, n, V[column], kr_);
+      launches_ += 1;
+      st = mg_apply(mixed);
+      if (!st) return st;
+      ++result.preconditioner_applies;
+      launch_copy(stream_, n, kz_, Z[column]);
+      launch_operator_shift(stream_, A, Z[column], V[column], kShift, w);
+      launches_ += 2;
+      ++result.operator_applies;
+      const int count = static_cast<int>(column) + 1;
+      st = multidot(count, true);
+      if (!st) return st;
+      double* column_h = h.data() + static_cast<size_t>(column) * rows;
+      for (int r = 0; r <= count; ++r) column_h[r] = h_scalars_->hcol[r];
+      const double bar_norm = column_h[count];
+      for (int r = 0; r < count; ++r) scales[r] = -column_h[r];
+      double t = bar_norm;
+      for (int r = 0; r < count; ++r) t = t - column_h[r] * column_h[r];
+      if (!std::isfinite(t)) {
+        result.termination = HFPS_NON_FINITE;
+        return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite Arnoldi norm");
+      }
+      const bool unsafe = t < 0.0;
+      double next_norm = unsafe ? 0.0 : std::sqrt(t);
+      if (unsafe && column != 0) {
+        // Discard the column and finish the cycle on the previous ones.
+        ++it;
+        result.iterations = it;
+        st = solve_y(static_cast<int>(column));
+        if (!st) return st;
+        basis_update(kx_, Z.data(), y.data(), static_cast<int>(column), 1.0, false, kx_);
+        double norm = 0.0;
+        st = true_residual(kx_, V[0], norm);
+        if (!st) return st;
+        result.final_true_residual = norm;
+        record(norm);
+        if (norm <= tol) {
+          result.termination = HFPS_CONVERGED;
+          return {};
+        }
+        if (it == control.maximum_iterations) break;
+        std::fill(h.begin(), h.end(), 0.0);
+        std::fill(cs.begin(), cs.end(), 0.0);
+        std::fill(sn.begin(), sn.end(), 0.0);
+        std::fill(g.begin(), g.end(), 0.0);
+        std::fill(y.begin(), y.end(), 0.0);
+        restarted = true;
+        break;
+      }
+      bool explicit_orth = false;
+      if (unsafe || next_norm == 0.0) {
+        // Second orthogonalisation pass, measured stably (:2330-2395).
+        basis_update(w, V.data(), scales.data(), count, 1.0, false, w);
+        st = multidot(count, false);
+        if (!st) return st;
+        for (int r = 0; r < count; ++r) {
+          const double c = h_scalars_->hcol[r];
+          column_h[r] += c;
+          scales[r] = -c;
+        }
+        basis_update(w, V.data(), scales.data(), count, 1.0, false, w);
+        launch_norm2(stream_, n, w, red(kOpMisc));
+        launches_ += 1;
+        st = sync_scalars();
+        if (!st) return st;
+        next_norm = std::sqrt(h_scalars_->misc[0]);
+        explicit_orth = true;
+      }
+      column_h[column] += kShift;
+      column_h[column + 1] = next_norm;
+      for (uint32_t r = 0; r < column; ++r) {
+        double& upper = h[static_cast<size_t>(column) * rows + r];
+        double& lower = h[static_cast<size_t>(column) * rows + r + 1];
+        const double rotated = cs[r] * upper + sn[r] * lower;
+        lower = -sn[r] * upper + cs[r] * lower;
+        upper = rotated;
+      }
+      double& diagonal = h[static_cast<size_t>(column) * rows + column];
+      double& subdiagonal = h[static_cast<size_t>(column) * rows + column + 1];
+      const double rotation_norm = std::hypot(diagonal, subdiagonal);
+      if (!(rotation_norm > 0.0) || !std::isfinite(rotation_norm)) {
+        result.termination = HFPS_BREAKDOWN;
+        return fail(HFPS_NUMERICAL_FAILURE, kDetailBreakdown, "FGMRES rotation breakdown");
+      }
+      cs[column] = diagonal / rotation_norm;
+      sn[column] = subdiagonal / rotation_norm;
+      diagonal = rotation_norm;
+      subdiagonal = 0.0;
+      g[column + 1] = -sn[column] * g[column];
+      g[column] = cs[column] * g[column];
+      ++it;
+      result.iterations = it;
+      const double recursive = std::abs(g[column + 1]);
+      record(recursive);
+      const bool happy = next_norm == 0.0;
+      const bool cycle_end = happy || column + 1 == restart || it == control.maximum_iterations;
+      const bool verify = happy || recursive <= tol ||
+                          it % control.true_residual_interval == 0 || cycle_end;
+      if (!cycle_end) {
+        // v_{j+1} = (w - sum h_r v_r) / |.|, one fused pass.
+        if (explicit_orth) basis_update(w, nullptr, nullptr, 0, 1.0 / next_norm, true, V[column + 1]);
+        else basis_update(w, V.data(), scales.data(), count, 1.0 / next_norm, true, V[column + 1]);
+      }
+      if (!verify) continue;
+      st = solve_y(count);
+      if (!st) return st;
+      if (!cycle_end) {
+        // Audit the candidate x + Z y in the unused last basis slot.
+        double* trial = V[restart];
+        basis_update(kx_, Z.data(), y.data(), count, 1.0, false, trial);
+        double audited = 0.0;
+        st = true_residual(trial, w, audited);
+        if (!st) return st;
+        result.final_true_residual = audited;
+        if (audited <= tol) {
+          launch_copy(stream_, n, trial, kx_);
+          launches_ += 1;
+          result.termination = HFPS_CONVERGED;
+          return {};
+        }
+        continue;
+      }
+      basis_update(kx_, Z.data(), y.data(), count, 1.0, false, kx_);
+      double norm = 0.0;
+      st = true_residual(kx_, V[0], norm);
+      if (!st) return st;
+      result.final_true_residual = norm;
+      result.recursive_residual = norm;
+      if (norm <= tol) {
+        result.termination = HFPS_CONVERGED;
+        return {};
+      }
+      if (it == control.maximum_iterations) break;
+      if (happy) {
+        const double guard = 64.0 * std::numeric_limits<double>::epsilon() * std::max(beta, tol);
+        if (!(norm + guard < beta)) {
+          result.termination = HFPS_BREAKDOWN;
+          return fail(HFPS_NUMERICAL_FAILURE, kDetailBreakdown, "FGMRES stagnation");
+        }
+      }
+      restarted = true;
+      break;
+    }
+    if (!restarted) break;
+  }
+  result.termination = HFPS_MAXIMUM_ITERATIONS;
+  return fail(HFPS_REJECTED_STEP, kDetailBreakdown, "maximum iterations reached");
+}
+
 Status Solver::solve(const double* rhs, double* solution, int memory,
                      const hfps_control& control, hfps_result& result,
                      double* history, uint32_t capacity) {
@@ -849,16 +1174,18 @@ Status Solver::solve(const double* rhs, double* solution, int memory,
       !std::isfinite(control.absolute_tolerance) ||
       control.relative_tolerance < 0.0 || control.absolute_tolerance < 0.0 ||
       (control.relative_tolerance == 0.0 && control.absolute_tolerance == 0.0) ||
-      control.algorithm != HFPS_PCG ||
       (control.precision != HFPS_FP64 && control.precision != HFPS_MIXED) ||
-      control.restart != 0 || !policy_.unit_linear)
+      !((control.algorithm == HFPS_PCG && control.restart == 0 && policy_.unit_linear) ||
+        (control.algorithm == HFPS_FGMRES && control.restart >= 1 &&
+         control.restart <= static_cast<uint32_t>(kMaxFgmresRestart))))
     return fail(HFPS_INVALID_PLAN, kDetailPlan, "invalid solve control");
   const size_t n = static_cast<size_t>(nx_) * ny_ * nz_;
   Status st = copy_in(kb_, rhs, n, memory);
   if (st) st = copy_in(kx_, solution, n, memory);
   if (!st) return st;
   launches_ = 0;
-  st = krylov_pcg(control, result, history, capacity);
+  st = control.algorithm == HFPS_FGMRES ? krylov_fgmres(control, result, history, capacity)
+                                        : krylov_pcg(control, result, history, capacity);
   result.kernel_launches = launches_;
   if (st) {
     st = copy_out(solution, kx_, n, memory);

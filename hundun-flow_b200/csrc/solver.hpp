@@ -102,6 +102,9 @@ class Solver {
   void coarse_solve(std::vector<DeviceLevel<T>>& levels);
   Status krylov_pcg(const hfps_control& control, hfps_result& result,
                     double* history, uint32_t capacity);
+  Status krylov_fgmres(const hfps_control& control, hfps_result& result,
+                       double* history, uint32_t capacity);
+  Status ensure_fgmres_storage(uint32_t restart);
   Status sync_scalars();
   Status copy_in(double* dst, const double* src, size_t n, int memory);
   Status copy_out(double* dst, const double* src, size_t n, int memory);
@@ -147,6 +150,13 @@ class Solver {
   double* coarse_op_{};
   int coarse_axis_{-1};
   bool coarse_dense_{};
+  // FGMRES basis: V_0..V_restart, Z_0..Z_{restart-1} and the operator image,
+  // allocated on first use for the largest restart asked for.
+  double* fg_storage_{};
+  uint32_t fg_restart_{};
+  std::vector<double*> fg_v_;
+  std::vector<double*> fg_z_;
+  double* fg_w_{};
   cudaGraphExec_t mg_graph_[2]{};
   size_t mg_nodes_[2]{};      // kernels per MG application (graph nodes)
   uint64_t launches_{};       // kernels launched since the last reset

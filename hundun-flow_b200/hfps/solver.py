@@ -206,6 +206,8 @@ class SolveOptions:
     maxit: int = 400
     true_residual_interval: int = 4
     precision: int = FP64
+    algorithm: int = PCG   # PCG (solve_pcg) or FGMRES (solve_fgmres)
+    restart: int = 0       # FGMRES restart length (the reference's default is 12)
 
 
 class PressureSolver:
@@ -347,6 +349,10 @@ class PressureSolver:
         c.maximum_iterations = options.maxit
         c.true_residual_interval = options.true_residual_interval
         c.precision = options.precision
+        c.algorithm = options.algorithm
+        c.restart = options.restart if options.algorithm == FGMRES else 0
+        if options.algorithm == FGMRES and c.restart == 0:
+            c.restart = 12
         return c
 
     def solve(self, rhs, x0=None, options: Optional[SolveOptions] = None, out=None,

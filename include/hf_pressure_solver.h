@@ -175,9 +175,13 @@ HFPS_API int hfps_set_beta(hfps_solver* solver, const double* beta,
 /* solve(rhs, x0, tol) -> x, iterations, residual history.  Replaces
  * solve_pcg / solve_fgmres with NativeCartesianMgPlan as preconditioner
  * (include/hundun/v04_linear.hpp:1070-1088; src/solver_krylov.cpp:1299-1555,
- * 1557-2650).  `solution` holds x0 on entry and x on success; on failure it
- * is left unchanged.  `history` (may be NULL) receives the recursive
- * residual norm after every iteration, up to `history_capacity` values. */
+ * 1557-2650).  control->algorithm selects HFPS_PCG (restart 0; needs the
+ * unit_linear MG scaling, as solve_pcg needs a fixed SPD preconditioner) or
+ * HFPS_FGMRES (restart 1..64; either scaling, the reference's production
+ * choice being the residual-minimising one with restart 12).  `solution`
+ * holds x0 on entry and x on success; on failure it is left unchanged.
+ * `history` (may be NULL) receives the recursive residual norm after every
+ * iteration, up to `history_capacity` values. */
 HFPS_API int hfps_solve(hfps_solver* solver, const double* rhs, double* solution,
                int memory, const hfps_control* control, hfps_result* result,
                double* history, uint32_t history_capacity);

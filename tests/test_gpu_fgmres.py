@@ -1,0 +1,139 @@
+"""solve_fgmres on the GPU (through the C ABI) against the reference.
+
+The reference's production pressure solve is solve_fgmres(12) with the
+MG plan's residual-minimising correction scaling
+(src/solver_krylov.cpp:1557-2650; src/solver_mg.cpp:4977-5122).  Bars:
+* residual-minimising MG correction: 1e-13 relative to the reference's own
+  output for point smoothers (the scale alpha = (r.Az)/(Az.Az) is a ratio of
+  global sums that the reference forms with compensated sums and the GPU
+  with fixed-order FP64 trees; the unscaled cycle is bit-identical, see
+  test_gpu_parity.py), 1e-11 relative in line mode;
+* solves at 1e-13: iterations within +-20% of the reference's and p within
+  1e-9 relative L2 of its solution (golden fixtures); the same iteration and
+  operator-apply counts as the C restatement run in the GPU's zebra line
+  order, solution within 1e-12;
+* restart lengths below the iteration count (cycle-end restarts and interior
+  true-residual audits), restarts above the 16-vector chunk of one basis
+  launch, the mixed-precision form and the iteration cap.
+"""
+import numpy as np
+import pytest
+
+import golden_cases
+from hfps import workloads
+
+pytestmark = [pytest.mark.gpu, pytest.mark.usefixtures("oracle_built")]
+
+
+@pytest.fixture(scope="module")
+def hfps_mod(cuda_library):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU tests need a CUDA device")
+    import hfps
+    return hfps
+
+
+def gpu_policy(hfps, p, unit_linear=0):
+    return hfps.Policy.default().replace(
+        point_smoother=p.smoother, cycle=p.cycle, pre_sweeps=p.pre, post_sweeps=p.post,
+        coarse_sweeps=p.coarse_sweeps, maximum_levels=p.max_levels,
+        minimum_coarse_extent=p.min_coarse_extent,
+        chebyshev_lower_spectrum_fraction=p.chebyshev_fraction,
+        anisotropy_threshold=p.anisotropy_threshold,
+        diagonal_shortcut_maximum_ratio=p.diagonal_shortcut, unit_linear=unit_linear)
+
+
+def oracle(system, policy, line_order=1):
+    import c_oracle
+    return c_oracle.OracleSession(system, policy, unit_linear=False, line_order=line_order)
+
+
+def rel(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+CASES = sorted(golden_cases.index())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_residual_minimising_mg_matches(hfps_mod, name):
+    s = golden_cases.system(name)
+    pol = golden_cases.policy(name)
+    g = hfps_mod.PressureSolver.from_system(s, gpu_policy(hfps_mod, pol))
+    v = golden_cases.probe(s)
+    z = g.apply_preconditioner(v)
+    o = oracle(s, pol)
+    if any(l[3] for l in o.levels()):
+        assert rel(z, o.apply_mg(v)) <= 1e-11
+    else:
+        assert rel(z, golden_cases.arrays(name)["mg_residual_minimising"]) <= 1e-13
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_fgmres_parity_with_reference(hfps_mod, name):
+    s = golden_cases.system(name)
+    pol = golden_cases.policy(name)
+    meta = golden_cases.index()[name]
+    gold = golden_cases.arrays(name)
+    g = hfps_mod.PressureSolver.from_system(s, gpu_policy(hfps_mod, pol))
+    x, info = g.solve(s.rhs, rtol=1e-13, maxit=400, algorithm=hfps_mod.FGMRES, restart=12)
+    assert info["termination"] == "converged"
+    ref_it = meta["fgmres_iterations_1e13"]
+    assert abs(info["iterations"] - ref_it) <= max(1, int(0.2 * ref_it))
+    assert np.linalg.norm(x - gold["x_fgmres"]) / np.linalg.norm(gold["x_fgmres"]) <= 1e-9
+    xo, io = oracle(s, pol).solve(s.rhs, rtol=1e-13, maxit=400, algorithm="fgmres", restart=12)
+    assert info["iterations"] == io["iterations"]
+    assert info["operator_applies"] == io["operator_applies"]
+    assert info["preconditioner_applies"] == io["preconditioner_applies"]
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-12
+    assert len(info["history"]) == info["iterations"]
+
+
+@pytest.mark.parametrize("restart,tri", [(3, 4), (5, 2), (20, 4)])
+def test_fgmres_restarts_and_audits_match_restatement(hfps_mod, restart, tri):
+    import ref_oracle
+    s = workloads.make("sphere64", n=(24, 20, 16), seed=8)
+    pol = ref_oracle.MgPolicy()
+    g = hfps_mod.PressureSolver.from_system(s, gpu_policy(hfps_mod, pol))
+    x, info = g.solve(s.rhs, rtol=1e-12, maxit=400, true_residual_interval=tri,
+                      algorithm=hfps_mod.FGMRES, restart=restart)
+    xo, io = oracle(s, pol).solve(s.rhs, rtol=1e-12, maxit=400, true_residual_interval=tri,
+                                  algorithm="fgmres", restart=restart)
+    assert info["termination"] == io["termination"] == "converged"
+    assert (info["iterations"], info["operator_applies"]) == (io["iterations"],
+                                                              io["operator_applies"])
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) <= 1e-12
+
+
+def test_fgmres_mixed_precision_reaches_fp64_tolerance(hfps_mod):
+    s = workloads.make("sphere64", n=(48, 40, 36))
+    g = hfps_mod.PressureSolver.from_system(s, hfps_mod.Policy.production().replace(unit_linear=0))
+    x64, i64 = g.solve(s.rhs, rtol=1e-12, algorithm=hfps_mod.FGMRES, restart=12)
+    xm, im = g.solve(s.rhs, rtol=1e-12, algorithm=hfps_mod.FGMRES, restart=12,
+                     precision=hfps_mod.MIXED)
+    assert im["termination"] == "converged"
+    assert im["final_true_residual"] <= 1e-12 * im["rhs_norm"]
+    assert np.linalg.norm(xm - x64) / np.linalg.norm(x64) <= 1e-9
+
+
+def test_fgmres_iteration_cap_publishes_nothing(hfps_mod):
+    s = workloads.make("sphere64", n=(16, 16, 16))
+    g = hfps_mod.PressureSolver.from_system(s, hfps_mod.Policy.production().replace(unit_linear=0))
+    x0 = np.full_like(s.rhs, 0.25)
+    with pytest.raises(hfps_mod.SolverError) as err:
+        g.solve(s.rhs, x0=x0, out=x0, rtol=1e-14, maxit=5, algorithm=hfps_mod.FGMRES, restart=3)
+    assert err.value.status == 6
+    assert err.value.result["termination"] == "maximum_iterations"
+    assert err.value.result["iterations"] == 5
+    assert np.all(x0 == 0.25)
+
+
+def test_pcg_needs_unit_scaling(hfps_mod):
+    """solve_pcg requires a fixed SPD preconditioner: the residual-minimising
+    MG plan is rejected for PCG (validate_solve, src/solver_krylov.cpp:962-971)."""
+    s = workloads.make("sphere64", n=(8, 8, 8))
+    g = hfps_mod.PressureSolver.from_system(s, hfps_mod.Policy.production().replace(unit_linear=0))
+    with pytest.raises(hfps_mod.SolverError) as err:
+        g.solve(s.rhs)
+    assert err.value.status == 2
