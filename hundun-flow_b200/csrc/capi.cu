@@ -118,6 +118,21 @@ int hfps_set_beta(hfps_solver* s, const double* beta, const double* storage,
   return guarded(s, [&](hfps::Solver& v) { return v.set_beta(beta, storage, memory); });
 }
 
+int hfps_assemble(hfps_solver* s, const hfps_assembly* assembly, double* rhs, int memory) {
+  if (assembly == nullptr) return HFPS_INVALID_PLAN;
+  return guarded(s, [&](hfps::Solver& v) { return v.assemble(*assembly, rhs, memory); });
+}
+
+int hfps_correct_flux(hfps_solver* s, const double* correction, const double* coefficient_x,
+                      const double* coefficient_y, const double* coefficient_z,
+                      double correction_scale, double* flux_x, double* flux_y,
+                      double* flux_z, int memory) {
+  return guarded(s, [&](hfps::Solver& v) {
+    return v.correct_flux(correction, coefficient_x, coefficient_y, coefficient_z,
+                          correction_scale, flux_x, flux_y, flux_z, memory);
+  });
+}
+
 int hfps_solve(hfps_solver* s, const double* rhs, double* solution, int memory,
                const hfps_control* control, hfps_result* result,
                double* history, uint32_t history_capacity) {

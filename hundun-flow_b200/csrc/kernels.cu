@@ -925,6 +925,114 @@ __global__ void k_beta_diagonal(int nx, int ny, int nz, const double* fx,
   }
 }
 
+// Pressure-correction system (assemble_pressure_system_impl,
+// src/solver_pressure.cpp:110-332), one cell per thread, in the reference's
+// operation order:
+//   V      = w_x w_y w_z (cell_volume, src/solver_cartesian.cpp:333-337)
+//   defect = V ((a0 rho + a1 rho_n) + a2 rho_nm1 - S)
+//   diag   = (a0 V) psi + face_sum (x-, x+, y-, y+, z-, z+)
+//   rhs    = -(defect + outward_flux) (x+ - x- + y+ - y- + z+ - z-)
+// Any input the reference rejects (non-positive density, derivative, volume
+// or diagonal, a negative or non-finite face coefficient, a non-finite
+// result) sets flags bit 2; nothing is published then.
+__global__ void k_assemble(int nx, int ny, int nz, const double* xf, const double* yf,
+                           const double* zf, double a0, double a1, double a2, int bdf2,
+                           const double* rho, const double* rho_n, const double* rho_nm1,
+                           const double* psi, const double* source, const double* phix,
+                           const double* phiy, const double* phiz, const double* fx,
+                           const double* fy, const double* fz, double* diag, double* rhs,
+                           Scalars* scalars) {
+  grid_dependency_sync();
+  const int n = nx * ny * nz;
+  int bad = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, nx, ny, i, j, k);
+    const int fxi = c + j + ny * k;
+    const int fyi = c + nx * k;
+    const int plane = nx * ny;
+    const double volume = (xf[i + 1] - xf[i]) * (yf[j + 1] - yf[j]) * (zf[k + 1] - zf[k]);
+    const double r = rho[c];
+    const double rn = rho_n[c];
+    const double rnm1 = bdf2 ? rho_nm1[c] : 0.0;
+    const double derivative = psi[c];
+    const double s = source != nullptr ? source[c] : 0.0;
+    const double defect = volume * (a0 * r + a1 * rn + a2 * rnm1 - s);
+    const double f0 = fx[fxi], f1 = fx[fxi + 1], f2 = fy[fyi], f3 = fy[fyi + nx];
+    const double f4 = fz[c], f5 = fz[c + plane];
+    const double d = a0 * volume * derivative + (f0 + f1 + f2 + f3 + f4 + f5);
+    const double outward = phix[fxi + 1] - phix[fxi] + phiy[fyi + nx] - phiy[fyi] +
+                           phiz[c + plane] - phiz[c];
+    const double b = -(defect + outward);
+    const bool faces_ok = f0 >= 0.0 && f1 >= 0.0 && f2 >= 0.0 && f3 >= 0.0 && f4 >= 0.0 &&
+                          f5 >= 0.0 && isfinite(f0 + f1 + f2 + f3 + f4 + f5);
+    if (!(r > 0.0) || !(rn > 0.0) || (bdf2 && !(rnm1 > 0.0)) || !(derivative > 0.0) ||
+        !(volume > 0.0) || !(d > 0.0) || !isfinite(defect) || !isfinite(d) ||
+        !isfinite(b) || !faces_ok)
+      bad = 1;
+    diag[c] = d;
+    rhs[c] = b;
+  }
+  if (bad) atomicOr(&scalars->flags, 4);
+}
+
+// Mass-flux response of a pressure correction (mass_flux_response,
+// src/solver_piso.cpp:1605-1653): flux_f += -c_f * (scale * jump_f) with
+// jump = p'_right - p'_left inside, +p'_cell on a low Dirichlet boundary
+// face, -p'_cell on a high one, 0 on Neumann faces; scale 1 applies the jump
+// unscaled.  One face per thread over the x, y and z face arrays.
+__global__ void k_correct_flux(int nx, int ny, int nz, unsigned neumann,
+                               const double* p, const double* cx, const double* cy,
+                               const double* cz, double scale, double* qx, double* qy,
+                               double* qz, Scalars* scalars) {
+  grid_dependency_sync();
+  const int nfx = (nx + 1) * ny * nz;
+  const int nfy = nx * (ny + 1) * nz;
+  const int nfz = nx * ny * (nz + 1);
+  const int total = nfx + nfy + nfz;
+  int bad = 0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += gridDim.x * blockDim.x) {
+    int axis, f, face, extent, cell_hi, step;
+    if (t < nfx) {
+      axis = 0; f = t; extent = nx;
+      const int row = f / (nx + 1);
+      face = f - row * (nx + 1);
+      cell_hi = face + nx * row;
+      step = 1;
+    } else if (t < nfx + nfy) {
+      axis = 1; f = t - nfx; extent = ny;
+      const int i = f % nx;
+      const int r = f / nx;
+      const int k = r / (ny + 1);
+      face = r - k * (ny + 1);
+      cell_hi = i + nx * (face + ny * k);
+      step = nx;
+    } else {
+      axis = 2; f = t - nfx - nfy; extent = nz;
+      face = f / (nx * ny);
+      cell_hi = f;
+      step = nx * ny;
+    }
+    double jump;
+    if (face == 0) {
+      jump = ((neumann >> (2 * axis)) & 1u) ? 0.0 : p[cell_hi];
+    } else if (face == extent) {
+      jump = ((neumann >> (2 * axis + 1)) & 1u) ? 0.0 : -p[cell_hi - step];
+    } else {
+      jump = p[cell_hi] - p[cell_hi - step];
+    }
+    const double applied = scale == 1.0 ? jump : scale * jump;
+    double* q = axis == 0 ? qx : (axis == 1 ? qy : qz);
+    const double* coefficient = axis == 0 ? cx : (axis == 1 ? cy : cz);
+    const double next = q[f] + -coefficient[f] * applied;
+    bad |= !isfinite(next);
+    q[f] = next;
+  }
+  if (bad) atomicOr(&scalars->flags, 1);
+}
+
 __global__ void k_shortcut_ratio(Level<double> L, Reduce red) {
   grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
@@ -1190,6 +1298,27 @@ void launch_beta_coefficients(cudaStream_t s, int nx, int ny, int nz,
                                                     z_faces, neumann, beta, fx, fy,
                                                     fz);
   launch(k_beta_diagonal, grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s, nx, ny, nz, fx, fy, fz, storage, diag);
+}
+void launch_assemble(cudaStream_t s, int nx, int ny, int nz, const double* xf,
+                     const double* yf, const double* zf, double a0, double a1, double a2,
+                     bool bdf2, const double* rho, const double* rho_n, const double* rho_nm1,
+                     const double* psi, const double* source, const double* phix,
+                     const double* phiy, const double* phiz, const double* fx,
+                     const double* fy, const double* fz, double* diag, double* rhs,
+                     Scalars* scalars) {
+  launch(k_assemble, grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s, nx, ny,
+         nz, xf, yf, zf, a0, a1, a2, bdf2 ? 1 : 0, rho, rho_n, rho_nm1, psi, source, phix,
+         phiy, phiz, fx, fy, fz, diag, rhs, scalars);
+}
+void launch_correct_flux(cudaStream_t s, int nx, int ny, int nz, unsigned neumann,
+                         const double* p, const double* cx, const double* cy,
+                         const double* cz, double scale, double* qx, double* qy, double* qz,
+                         Scalars* scalars) {
+  const long long faces = static_cast<long long>(nx + 1) * ny * nz +
+                          static_cast<long long>(nx) * (ny + 1) * nz +
+                          static_cast<long long>(nx) * ny * (nz + 1);
+  launch(k_correct_flux, grid_for(faces), kThreads, 0, s, nx, ny, nz, neumann, p, cx, cy, cz,
+         scale, qx, qy, qz, scalars);
 }
 void launch_shortcut_ratio(cudaStream_t s, const Level<double>& L,
                            Reduce red) {

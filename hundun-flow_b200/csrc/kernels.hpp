@@ -27,7 +27,7 @@ struct Scalars {
   double mg_alpha;   // MG correction scale
   double misc[4];
   double hcol[72];   // FGMRES: projections of the current column and |w|^2
-  int flags;         // bit 0 non-finite, bit 1 breakdown
+  int flags;         // bit 0 non-finite, bit 1 breakdown, bit 2 invalid assembly input
   unsigned counters[8];  // last-block arrival counters, one per reduction
 };
 
@@ -146,6 +146,21 @@ void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc);
 void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red);
 void launch_copy(cudaStream_t s, int n, const double* src, double* dst);
+// ---- the steps either side of the solve ----------------------------------------
+// Pressure-correction system assembly (diag, rhs) from densities, the
+// density derivative, the predicted face fluxes and the face coefficients.
+void launch_assemble(cudaStream_t s, int nx, int ny, int nz, const double* xf,
+                     const double* yf, const double* zf, double a0, double a1, double a2,
+                     bool bdf2, const double* rho, const double* rho_n, const double* rho_nm1,
+                     const double* psi, const double* source, const double* phix,
+                     const double* phiy, const double* phiz, const double* fx,
+                     const double* fy, const double* fz, double* diag, double* rhs,
+                     Scalars* scalars);
+// flux += mass-flux response of the correction p (in place).
+void launch_correct_flux(cudaStream_t s, int nx, int ny, int nz, unsigned neumann,
+                         const double* p, const double* cx, const double* cy,
+                         const double* cz, double scale, double* qx, double* qy, double* qz,
+                         Scalars* scalars);
 // ---- FGMRES (solve_fgmres) ---------------------------------------------------
 // Basis vectors handled by one multidot / basis-update launch.
 constexpr int kBasisChunk = 16;

@@ -549,6 +549,90 @@ Status Solver::set_beta(const double* beta, const double* storage, int memory) {
   return build_hierarchy();
 }
 
+Status Solver::assemble(const hfps_assembly& in, double* rhs, int memory) {
+  if (in.beta == nullptr || in.density_trial == nullptr || in.density_accepted == nullptr ||
+      in.drho_dp == nullptr || in.flux_x == nullptr || in.flux_y == nullptr ||
+      in.flux_z == nullptr || rhs == nullptr || (in.bdf_order != 1 && in.bdf_order != 2) ||
+      (in.bdf_order == 2 && in.density_previous == nullptr) || !std::isfinite(in.a0) ||
+      !std::isfinite(in.a1) || !std::isfinite(in.a2) || !(in.a0 > 0.0))
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "invalid assembly input");
+  const size_t cells = static_cast<size_t>(nx_) * ny_ * nz_;
+  const size_t nf[3] = {static_cast<size_t>(nx_ + 1) * ny_ * nz_,
+                        static_cast<size_t>(nx_) * (ny_ + 1) * nz_,
+                        static_cast<size_t>(nx_) * ny_ * (nz_ + 1)};
+  // Device staging: the Krylov vectors are free between solves.
+  double* beta = kz_;
+  double* rho = kx_;
+  double* rho_n = kr_;
+  double* rho_nm1 = in.bdf_order == 2 ? kp_ : nullptr;
+  double* psi = kap_;
+  double* source = in.mass_source != nullptr ? kb_ : nullptr;
+  Status st = copy_in(beta, in.beta, cells, memory);
+  if (st) st = copy_in(rho, in.density_trial, cells, memory);
+  if (st) st = copy_in(rho_n, in.density_accepted, cells, memory);
+  if (st && rho_nm1 != nullptr) st = copy_in(rho_nm1, in.density_previous, cells, memory);
+  if (st) st = copy_in(psi, in.drho_dp, cells, memory);
+  if (st && source != nullptr) st = copy_in(source, in.mass_source, cells, memory);
+  if (!st) return st;
+  // Face coefficients from beta (face_pressure_coefficient), then the
+  // predicted fluxes into the aggregation scratch (free outside a rebuild).
+  launch_beta_coefficients(stream_, nx_, ny_, nz_, d_faces_[0], d_faces_[1], d_faces_[2],
+                           neumann_, beta, nullptr, user_[0], user_[1], user_[2], user_[3]);
+  st = copy_in(agg_[0], in.flux_x, nf[0], memory);
+  if (st) st = copy_in(agg_[1], in.flux_y, nf[1], memory);
+  if (st) st = copy_in(agg_[2], in.flux_z, nf[2], memory);
+  if (!st) return st;
+  st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  double* assembled_rhs = beta;  // beta is consumed by the face coefficients
+  launch_assemble(stream_, nx_, ny_, nz_, d_faces_[0], d_faces_[1], d_faces_[2], in.a0, in.a1,
+                  in.a2, in.bdf_order == 2, rho, rho_n, rho_nm1, psi, source, agg_[0], agg_[1],
+                  agg_[2], user_[1], user_[2], user_[3], user_[0], assembled_rhs, d_scalars_);
+  st = sync_scalars();
+  if (!st) return st;
+  if (h_scalars_->flags & 4)
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "pressure assembly rejected its input");
+  DeviceLevel<double>& L0 = l64_[0];
+  launch_mask_finest(stream_, nx_, ny_, nz_, d_faces_[0], d_faces_[1], d_faces_[2],
+                     user_[0], user_[1], user_[2], user_[3], d_active_, L0.diag,
+                     L0.fx, L0.fy, L0.fz, volume_[0], fluid_[0]);
+  st = build_hierarchy();
+  if (!st) return st;
+  st = copy_out(rhs, assembled_rhs, cells, memory);
+  if (!st) return st;
+  return check(cudaStreamSynchronize(stream_), "assembly");
+}
+
+Status Solver::correct_flux(const double* correction, const double* cx, const double* cy,
+                            const double* cz, double scale, double* qx, double* qy,
+                            double* qz, int memory) {
+  if (correction == nullptr || cx == nullptr || cy == nullptr || cz == nullptr ||
+      qx == nullptr || qy == nullptr || qz == nullptr || !std::isfinite(scale))
+    return fail(HFPS_INVALID_PLAN, kDetailPlan, "invalid flux-correction input");
+  const size_t cells = static_cast<size_t>(nx_) * ny_ * nz_;
+  const size_t nf[3] = {static_cast<size_t>(nx_ + 1) * ny_ * nz_,
+                        static_cast<size_t>(nx_) * (ny_ + 1) * nz_,
+                        static_cast<size_t>(nx_) * ny_ * (nz_ + 1)};
+  const double* c[3] = {cx, cy, cz};
+  double* q[3] = {qx, qy, qz};
+  // Staging: correction in kp_, coefficients in user_[1..3], fluxes in agg_.
+  Status st = copy_in(kp_, correction, cells, memory);
+  for (int a = 0; a < 3 && st; ++a) st = copy_in(user_[1 + a], c[a], nf[a], memory);
+  for (int a = 0; a < 3 && st; ++a) st = copy_in(agg_[a], q[a], nf[a], memory);
+  if (!st) return st;
+  st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  launch_correct_flux(stream_, nx_, ny_, nz_, neumann_, kp_, user_[1], user_[2], user_[3],
+                      scale, agg_[0], agg_[1], agg_[2], d_scalars_);
+  st = sync_scalars();
+  if (!st) return st;
+  if (h_scalars_->flags & 1)
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite corrected flux");
+  for (int a = 0; a < 3 && st; ++a) st = copy_out(q[a], agg_[a], nf[a], memory);
+  if (!st) return st;
+  return check(cudaStreamSynchronize(stream_), "flux correction");
+}
+
 // ---------------------------------------------------------------------------
 // MG cycle (mg_cycle, src/solver_mg.cpp:4192-4338).
 

@@ -62,6 +62,10 @@ class Solver {
   Status set_coefficients(const double* diag, const double* fx,
                           const double* fy, const double* fz, int memory);
   Status set_beta(const double* beta, const double* storage, int memory);
+  Status assemble(const hfps_assembly& in, double* rhs, int memory);
+  Status correct_flux(const double* correction, const double* cx, const double* cy,
+                      const double* cz, double scale, double* qx, double* qy, double* qz,
+                      int memory);
   Status solve(const double* rhs, double* solution, int memory,
                const hfps_control& control, hfps_result& result,
                double* history, uint32_t history_capacity);

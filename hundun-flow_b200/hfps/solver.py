@@ -110,6 +110,16 @@ class Result(ctypes.Structure):
         return d
 
 
+class Assembly(ctypes.Structure):
+    """hfps_assembly (PressureCorrectionInput)."""
+    _fields_ = [("bdf_order", ctypes.c_int), ("a0", ctypes.c_double), ("a1", ctypes.c_double),
+                ("a2", ctypes.c_double), ("beta", ctypes.c_void_p),
+                ("density_trial", ctypes.c_void_p), ("density_accepted", ctypes.c_void_p),
+                ("density_previous", ctypes.c_void_p), ("drho_dp", ctypes.c_void_p),
+                ("mass_source", ctypes.c_void_p), ("flux_x", ctypes.c_void_p),
+                ("flux_y", ctypes.c_void_p), ("flux_z", ctypes.c_void_p)]
+
+
 class OperatorView(ctypes.Structure):
     """hfps_operator_view: device coefficient arrays of the finest level."""
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
@@ -121,7 +131,8 @@ class OperatorView(ctypes.Structure):
 _LIB = None
 
 EXPORTS = ["hfps_default_policy", "hfps_production_policy", "hfps_default_control",
-           "hfps_create", "hfps_set_coefficients", "hfps_set_beta", "hfps_solve",
+           "hfps_create", "hfps_set_coefficients", "hfps_set_beta", "hfps_assemble",
+           "hfps_correct_flux", "hfps_solve",
            "hfps_apply_operator", "hfps_apply_preconditioner", "hfps_adjoint",
            "hfps_levels", "hfps_level_coefficients", "hfps_profile_kernel",
            "hfps_operator_dot_noalloc", "hfps_last_error", "hfps_destroy"]
@@ -145,6 +156,9 @@ def _lib():
                                     ctypes.POINTER(vp)]
         lib.hfps_set_coefficients.argtypes = [vp, vp, vp, vp, vp, ctypes.c_int]
         lib.hfps_set_beta.argtypes = [vp, vp, vp, ctypes.c_int]
+        lib.hfps_assemble.argtypes = [vp, ctypes.POINTER(Assembly), vp, ctypes.c_int]
+        lib.hfps_correct_flux.argtypes = [vp, vp, vp, vp, vp, ctypes.c_double, vp, vp, vp,
+                                          ctypes.c_int]
         lib.hfps_solve.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.POINTER(Control),
                                    ctypes.POINTER(Result), vp, ctypes.c_uint32]
         lib.hfps_apply_operator.argtypes = [vp, vp, vp, ctypes.c_int]
@@ -289,6 +303,43 @@ class PressureSolver:
         ps, ms = _ptr(storage, self.cells)
         memory = _same_memory(mb, ms if storage is not None else None)
         self._check(self._lib.hfps_set_beta(self._handle, pb, ps, memory), "set_beta")
+
+    def assemble(self, beta, density_trial, density_accepted, drho_dp, fluxes, a0, a1=0.0,
+                 a2=0.0, density_previous=None, mass_source=None, rhs=None):
+        """Assembles the pressure-correction system on the device (hfps_assemble),
+        makes it the solver's operator and returns rhs.  ``fluxes`` are the three
+        predicted face-flux arrays; BDF2 when ``density_previous`` is given."""
+        cells = [beta, density_trial, density_accepted, drho_dp]
+        ptrs = [_ptr(a, self.cells) for a in cells]
+        prev = _ptr(density_previous, self.cells)
+        src = _ptr(mass_source, self.cells)
+        flux = [_ptr(f, n) for f, n in zip(fluxes, self.face_counts)]
+        out = rhs if rhs is not None else self._like(beta)
+        po = _ptr(out, self.cells)
+        memory = _same_memory(*(m for _, m in ptrs), *(m for _, m in flux), po[1],
+                              prev[1] if density_previous is not None else None,
+                              src[1] if mass_source is not None else None)
+        a = Assembly()
+        a.bdf_order = 2 if density_previous is not None else 1
+        a.a0, a.a1, a.a2 = a0, a1, a2
+        a.beta, a.density_trial, a.density_accepted, a.drho_dp = (p for p, _ in ptrs)
+        a.density_previous = prev[0]
+        a.mass_source = src[0]
+        a.flux_x, a.flux_y, a.flux_z = (p for p, _ in flux)
+        self._check(self._lib.hfps_assemble(self._handle, ctypes.byref(a), po[0], memory),
+                    "assemble")
+        return out
+
+    def correct_flux(self, correction, coefficients, fluxes, scale=1.0):
+        """fluxes[axis] += mass-flux response of ``correction`` (in place)."""
+        pc = _ptr(correction, self.cells)
+        cs = [_ptr(c, n) for c, n in zip(coefficients, self.face_counts)]
+        qs = [_ptr(q, n) for q, n in zip(fluxes, self.face_counts)]
+        memory = _same_memory(pc[1], *(m for _, m in cs), *(m for _, m in qs))
+        self._check(self._lib.hfps_correct_flux(self._handle, pc[0], *(p for p, _ in cs),
+                                                scale, *(p for p, _ in qs), memory),
+                    "correct_flux")
+        return fluxes
 
     def levels(self):
         shapes = (ctypes.c_int * 128)()

@@ -172,6 +172,50 @@ HFPS_API int hfps_set_coefficients(hfps_solver* solver, const double* diagonal,
 HFPS_API int hfps_set_beta(hfps_solver* solver, const double* beta,
                   const double* storage, int memory);
 
+/* Inputs of the pressure-correction assembly (PressureCorrectionInput,
+ * src/solver_pressure.cpp:110-332).  Cell arrays are nx*ny*nz values, flux
+ * arrays the face extents; all in the memory the call names. */
+typedef struct hfps_assembly {
+  int bdf_order;                  /* 1 or 2 */
+  double a0, a1, a2;              /* BDF coefficients, a0 > 0 */
+  const double* beta;             /* cell beta for face_pressure_coefficient */
+  const double* density_trial;    /* rho^*, > 0 */
+  const double* density_accepted; /* rho^n, > 0 */
+  const double* density_previous; /* rho^{n-1} (BDF2 only; NULL for BDF1) */
+  const double* drho_dp;          /* d rho / d p at constant h, Y; > 0 */
+  const double* mass_source;      /* NULL = none */
+  const double* flux_x;           /* predicted face mass fluxes phi_HbyA */
+  const double* flux_y;
+  const double* flux_z;
+} hfps_assembly;
+
+/* Assembles the pressure-correction system on the device and makes it the
+ * solver's operator: face coefficients from beta (face_pressure_coefficient,
+ * src/solver_piso.cpp:1060-1136), then per cell, in the reference's order,
+ * diag = a0 V drho_dp + sum of the six face coefficients and
+ * rhs = -(V (a0 rho + a1 rho_n + a2 rho_{n-1} - S) + outward flux)
+ * (assemble_pressure_system_impl, src/solver_pressure.cpp:110-332), then
+ * the IBM masking and coarse levels as hfps_set_coefficients.  Writes rhs.
+ * Inputs the reference rejects (non-positive densities, derivative, volume
+ * or diagonal; negative or non-finite faces; non-finite results) return
+ * HFPS_NUMERICAL_FAILURE and change nothing. */
+HFPS_API int hfps_assemble(hfps_solver* solver, const hfps_assembly* assembly,
+                           double* rhs, int memory);
+
+/* Post-solve flux correction: flux_f += -c_f * (scale * jump_f(correction))
+ * on every face, jump = p'_R - p'_L inside, the owner cell's value (negated
+ * on a high face) at a Dirichlet boundary face and 0 at a Neumann one
+ * (PressureCorrectionBoundaryPlan::mass_flux_response, src/solver_piso.cpp:
+ * 1605-1653, as applied over all faces at :7400-7420).  coefficient_* are
+ * the pressure face coefficients the caller assembled with; flux_* are
+ * updated in place. */
+HFPS_API int hfps_correct_flux(hfps_solver* solver, const double* correction,
+                               const double* coefficient_x,
+                               const double* coefficient_y,
+                               const double* coefficient_z,
+                               double correction_scale, double* flux_x,
+                               double* flux_y, double* flux_z, int memory);
+
 /* solve(rhs, x0, tol) -> x, iterations, residual history.  Replaces
  * solve_pcg / solve_fgmres with NativeCartesianMgPlan as preconditioner
  * (include/hundun/v04_linear.hpp:1070-1088; src/solver_krylov.cpp:1299-1555,
