@@ -46,7 +46,7 @@ def _load():
                                   ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int]
         lib.hfo_solve_fgmres.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_int,
-                                         ctypes.c_int, dp, dp, ctypes.c_int]
+                                         ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int]
         _lib = lib
     return _lib
 
@@ -137,18 +137,20 @@ class OracleSession:
         return z
 
     def solve(self, rhs, x0: Optional[np.ndarray] = None, rtol=1e-10, atol=0.0, maxit=400,
-              true_residual_interval=4, algorithm: str = "pcg", restart: int = 12):
+              true_residual_interval=4, algorithm: str = "pcg", restart: int = 12,
+              recycle: str = "none"):
         """solve_pcg, or solve_fgmres(restart) when ``algorithm == "fgmres"``
         (build the session with unit_linear=False for the reference's
-        residual-minimising MG scaling)."""
+        residual-minimising MG scaling).  ``recycle`` as RefSession.solve."""
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         x = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64, order="C")
-        out = np.zeros(8)
+        out = np.zeros(13)
         hist = np.zeros(maxit)
         if algorithm == "fgmres":
+            modes = {"none": 0, "capture": 1, "project": 2, "guard": 3}
             rc = self._lib.hfo_solve_fgmres(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
-                                            true_residual_interval, restart, _dp(out), _dp(hist),
-                                            maxit)
+                                            true_residual_interval, restart, modes[recycle],
+                                            _dp(out), _dp(hist), maxit)
         else:
             rc = self._lib.hfo_solve(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
                                      true_residual_interval, _dp(out), _dp(hist), maxit)
@@ -164,5 +166,10 @@ class OracleSession:
             "operator_applies": int(out[6]),
             "preconditioner_applies": int(out[7]),
             "history": hist[:it].copy(),
+            "recycle_offered": int(out[8]),
+            "recycle_retained": int(out[9]),
+            "recycle_accepted": bool(out[10]),
+            "recycle_projected_residual": out[11],
+            "recycle_cycle_corrections": int(out[12]),
         }
         return x, info

@@ -52,6 +52,14 @@ typedef struct {
   double cheb_fraction, anisotropy, shortcut_ratio;
   int diagonal_shortcut;
   double* work[6];
+  /* FGMRES subspace recycling across solves (SolverWorkspace recycle state,
+   * src/solver_linear_state.cpp:735-1037): a ring of up to RECYCLE_MAX
+   * cycle corrections, oldest first from rc_oldest, and the cycle-start
+   * snapshot of x. */
+  int rc_capture, rc_guard_only, rc_cycle_active, rc_pending;
+  int rc_count, rc_oldest;
+  double* rc_ring[4];
+  double* rc_snapshot;
 } oracle_t;
 
 static size_t idx(const int* n, int i, int j, int k) {
@@ -913,16 +921,73 @@ static int back_substitute(const double* h, const double* g, double* y, int coun
   return -1;
 }
 
+#define RECYCLE_MAX 4
+
+static void recycle_clear(oracle_t* o) {
+  o->rc_capture = o->rc_guard_only = o->rc_cycle_active = o->rc_pending = 0;
+  o->rc_count = o->rc_oldest = 0;
+}
+
+static double* recycle_slot(oracle_t* o, int logical) {
+  return o->rc_ring[(o->rc_oldest + logical) % RECYCLE_MAX];
+}
+
+/* recycle_capture_cycle_start (src/solver_linear_state.cpp:857-895). */
+static void recycle_cycle_start(oracle_t* o, const double* x, size_t n) {
+  if (!o->rc_capture) return;
+  memcpy(o->rc_snapshot, x, n * sizeof(double));
+  o->rc_cycle_active = 1;
+}
+
+/* recycle_capture_cycle_publish (:897-1017): correction = x - snapshot;
+ * a nonzero one enters the ring, replacing the oldest when it is full. */
+static void recycle_publish(oracle_t* o, const double* x, size_t n, long* published) {
+  if (!o->rc_capture || !o->rc_cycle_active) return;
+  int nonzero = 0;
+  for (size_t c = 0; c < n; ++c) {
+    const double v = x[c] - o->rc_snapshot[c];
+    nonzero = nonzero || v != 0.0;
+    o->rc_snapshot[c] = v;
+  }
+  o->rc_cycle_active = 0;
+  if (!nonzero) return;
+  ++*published;
+  double* slot;
+  if (o->rc_count < RECYCLE_MAX) {
+    slot = o->rc_ring[(o->rc_oldest + o->rc_count) % RECYCLE_MAX];
+    ++o->rc_count;
+  } else {
+    slot = o->rc_ring[o->rc_oldest];
+    o->rc_oldest = (o->rc_oldest + 1) % RECYCLE_MAX;
+  }
+  memcpy(slot, o->rc_snapshot, n * sizeof(double));
+}
+
 int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
-                     double atol, int maxit, int tri, int restart, double* out,
-                     double* history, int hcap) {
+                     double atol, int maxit, int tri, int restart, int recycle,
+                     double* out, double* history, int hcap) {
   oracle_t* o = handle;
   const size_t n = o->lv[0].cells;
+  long rc_published = 0, rc_offered = 0, rc_retained = 0, rc_accepted = 0;
+  double rc_projected = 0.0;
+  if (o->rc_snapshot == NULL) {
+    o->rc_snapshot = calloc(n, sizeof(double));
+    for (int r = 0; r < RECYCLE_MAX; ++r) o->rc_ring[r] = calloc(n, sizeof(double));
+  }
+  /* Session selection as PressureVelocityCoupler makes it
+   * (src/solver_piso.cpp:10410-10433). */
+  if (recycle == 0) recycle_clear(o);
+  else if (recycle == 1) { recycle_clear(o); o->rc_capture = 1; }
+  else if (recycle == 2) {
+    if (!o->rc_capture || o->rc_cycle_active || o->rc_pending) { out[3] = TERM_BREAKDOWN; return 2; }
+    o->rc_capture = 0;
+    o->rc_pending = 1;
+  } else if (recycle == 3) { recycle_clear(o); o->rc_guard_only = 1; }
   int ok = 1;
   long op_applies = 0, pc_applies = 0;
   int it = 0;
   int term = TERM_MAXIMUM, status = 6;
-  memset(out, 0, 8 * sizeof(double));
+  memset(out, 0, 13 * sizeof(double));
   if (restart < 1 || restart > 64) { out[3] = TERM_BREAKDOWN; return 2; }
   const int rows = restart + 1;
   double** V = calloc((size_t)rows, sizeof(double*));
@@ -957,12 +1022,93 @@ int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
     dst_norm = norm2(V[0], n, &ok);                                        \
   } while (0)
   TRUE_RESIDUAL(initial, x);
+  /* reset_to_zero_initial_guess under the recycle guard (:1673-1686). */
+  if ((o->rc_capture || o->rc_guard_only) && initial > bnorm) {
+    for (size_t c = 0; c < n; ++c) { x[c] = 0.0; V[0][c] = rhs[c]; }
+    initial = bnorm;
+  }
   final_true = initial;
   recursive = initial;
   if (!ok) { term = TERM_NON_FINITE; status = 5; goto done; }
-  if (initial <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+  if (initial <= tol) { o->rc_pending = 0; term = TERM_CONVERGED; status = 0; goto done; }
   int deferred = 0;
+  if (o->rc_pending) {
+    /* apply_recycle_projection (src/solver_krylov.cpp:1745-2019): images
+     * A d_i, two classical Gram-Schmidt passes against the retained images
+     * (directions follow), normalisation, alpha_i = image_i . r, and the
+     * candidate x + sum alpha_i d_i accepted if its true residual is lower.
+     * The projection's operator applies are not counted as the solve's. */
+    o->rc_pending = 0;
+    const int offered = o->rc_count;
+    rc_offered = offered;
+    double* images[RECYCLE_MAX];
+    double* dirs[RECYCLE_MAX];
+    double pre[RECYCLE_MAX];
+    int kept[RECYCLE_MAX];
+    double max_pre = 0.0;
+    for (int i = 0; i < offered; ++i) {
+      dirs[i] = recycle_slot(o, i);
+      /* workspace slot v_begin + 1 + i: basis slots, then the (still free)
+       * preconditioned-basis slots when the restart is short */
+      images[i] = 1 + i < rows ? V[1 + i] : Z[1 + i - rows];
+      hfo_apply_operator(o, dirs[i], images[i]);
+      pre[i] = norm2(images[i], n, &ok);
+      if (pre[i] > max_pre) max_pre = pre[i];
+    }
+    int retained = 0;
+    if (offered > 0 && max_pre > 0.0 && isfinite(max_pre)) {
+      const double threshold = 64.0 * DBL_EPSILON * max_pre;
+      for (int i = 0; i < offered; ++i) {
+        if (!(pre[i] > threshold)) continue;
+        double image_norm = pre[i];
+        if (retained != 0) {
+          for (int pass = 0; pass < 2; ++pass) {
+            double dots[RECYCLE_MAX];
+            for (int p = 0; p < retained; ++p) dots[p] = dot(images[kept[p]], images[i], n, &ok);
+            for (int p = 0; p < retained; ++p) {
+              const double coefficient = dots[p];
+              for (size_t c = 0; c < n; ++c)
+                images[i][c] = images[i][c] + -coefficient * images[kept[p]][c];
+              for (size_t c = 0; c < n; ++c)
+                dirs[i][c] = dirs[i][c] + -coefficient * dirs[kept[p]][c];
+            }
+          }
+          image_norm = norm2(images[i], n, &ok);
+        }
+        if (!(image_norm > threshold) || !isfinite(image_norm)) continue;
+        const double inverse = 1.0 / image_norm;
+        for (size_t c = 0; c < n; ++c) images[i][c] = inverse * images[i][c];
+        for (size_t c = 0; c < n; ++c) dirs[i][c] = inverse * dirs[i][c];
+        kept[retained++] = i;
+      }
+    }
+    rc_retained = retained;
+    if (retained > 0) {
+      double alpha[RECYCLE_MAX];
+      for (int p = 0; p < retained; ++p) alpha[p] = dot(images[kept[p]], V[0], n, &ok);
+      double* candidate = o->rc_snapshot;
+      memcpy(candidate, x, n * sizeof(double));
+      for (int p = 0; p < retained; ++p)
+        for (size_t c = 0; c < n; ++c)
+          candidate[c] = candidate[c] + alpha[p] * dirs[kept[p]][c];
+      hfo_apply_operator(o, candidate, ax);
+      for (size_t c = 0; c < n; ++c) ax[c] = 1.0 * rhs[c] + -1.0 * ax[c];
+      const double candidate_norm = norm2(ax, n, &ok);
+      rc_projected = candidate_norm;
+      if (isfinite(candidate_norm) && candidate_norm < final_true) {
+        memcpy(x, candidate, n * sizeof(double));
+        memcpy(V[0], ax, n * sizeof(double));
+        final_true = candidate_norm;
+        recursive = candidate_norm;
+        rc_accepted = 1;
+        if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+      }
+    }
+    o->rc_count = 0;
+    o->rc_oldest = 0;
+  }
   while (it < maxit) {
+    recycle_cycle_start(o, x, n);
     const double beta = final_true;
     const double inv_beta = 1.0 / beta;
     for (size_t c = 0; c < n; ++c) V[0][c] = inv_beta * V[0][c];
@@ -1002,6 +1148,7 @@ int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
         if (bs >= 0) { term = bs; status = 5; goto done; }
         if (!add_scaled_basis(x, Z, y, valid, n)) { term = TERM_NON_FINITE; status = 5; goto done; }
         TRUE_RESIDUAL(final_true, x);
+        recycle_publish(o, x, n, &rc_published);
         recursive = final_true;
         if (history && it - 1 < hcap) history[it - 1] = recursive;
         if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
@@ -1075,6 +1222,7 @@ int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
         const double audited = norm2(ax, n, &ok);
         final_true = audited;
         if (audited <= tol) {
+          recycle_publish(o, trial, n, &rc_published);
           memcpy(x, trial, n * sizeof(double));
           term = TERM_CONVERGED; status = 0; goto done;
         }
@@ -1082,6 +1230,7 @@ int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
       }
       add_scaled_basis(x, Z, y, count, n);
       TRUE_RESIDUAL(final_true, x);
+      recycle_publish(o, x, n, &rc_published);
       recursive = final_true;
       if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
       if (it == maxit) { term = TERM_MAXIMUM; status = 6; goto done; }
@@ -1102,6 +1251,11 @@ done:
   out[3] = term;
   out[6] = (double)op_applies;
   out[7] = (double)pc_applies;
+  out[8] = (double)rc_offered;
+  out[9] = (double)rc_retained;
+  out[10] = (double)rc_accepted;
+  out[11] = rc_projected;
+  out[12] = (double)rc_published;
   for (int i = 0; i < rows; ++i) free(V[i]);
   for (int i = 0; i < restart; ++i) free(Z[i]);
   free(V); free(Z); free(ax); free(h); free(cs); free(sn); free(g); free(y);
@@ -1178,6 +1332,8 @@ void hfo_destroy(void* handle) {
   }
   for (int a = 0; a < 3; ++a) free(o->faces[a]);
   for (int w = 0; w < 6; ++w) free(o->work[w]);
+  for (int r = 0; r < 4; ++r) free(o->rc_ring[r]);
+  free(o->rc_snapshot);
   free(o->diag0); free(o->fx0); free(o->fy0); free(o->fz0); free(o->active);
   free(o);
 }

@@ -48,12 +48,15 @@ int hfo_solve(void* handle, const double* rhs, double* x,
               double* outputs, double* history, int history_capacity);
 
 /* solve_fgmres (src/solver_krylov.cpp:1557-2650) with the MG plan as the
- * (flexible) preconditioner; same outputs and history as hfo_solve. */
+ * (flexible) preconditioner.  recycle: 0 none, 1 capture cycle corrections
+ * for the next solve, 2 project the captured ones, 3 initial-guess guard
+ * only.  outputs (13): hfo_solve's eight, then recycle offered, retained,
+ * accepted, projected residual, corrections captured by this solve. */
 int hfo_solve_fgmres(void* handle, const double* rhs, double* x,
                      double relative_tolerance, double absolute_tolerance,
                      int maximum_iterations, int true_residual_interval,
-                     int restart, double* outputs, double* history,
-                     int history_capacity);
+                     int restart, int recycle, double* outputs,
+                     double* history, int history_capacity);
 
 #ifdef __cplusplus
 }

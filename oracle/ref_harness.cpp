@@ -485,14 +485,38 @@ int hfref_apply_mg(void* handle, const double* r, double* z) {
 }
 
 // Runs solve_pcg (adapter-certified MG) or solve_fgmres (MG as given).
+// recycle (FGMRES): 0 none (clears any recycle session), 1 begin a capture
+// session (corrector 1: SolverWorkspace::recycle_begin_capture), 2 project
+// the captured corrections (corrector 2: recycle_begin_projection), 3 the
+// zero-seed initial-guess guard only (recycle_begin_initial_guess_guard),
+// as PressureVelocityCoupler selects them (src/solver_piso.cpp:10410-10433),
+// through the reference's test-access entry points.
 // outputs: [iterations, initial_true, final_true, termination, rhs_norm,
 //           limit, operator_applies, preconditioner_applies, seconds,
-//           setup_seconds]
+//           setup_seconds, recycle_offered, recycle_retained,
+//           recycle_accepted, recycle_projected_residual,
+//           recycle_cycle_corrections]
 int hfref_solve(void* handle, const double* rhs, double* solution,
                 double relative_tolerance, double absolute_tolerance,
                 int maximum_iterations, int true_residual_interval,
-                double* outputs) {
+                int recycle, double* outputs) {
   Session& s = *static_cast<Session*>(handle);
+  if (s.algorithm == LinearAlgorithm::fgmres) {
+    Status rs{};
+    if (recycle == 0) {
+      s.workspace.recycle_clear_for_test();
+    } else if (recycle == 1) {
+      s.workspace.recycle_clear_for_test();
+      rs = s.workspace.recycle_begin_capture_for_test(s.cells, s.identity.fingerprint);
+    } else if (recycle == 2) {
+      rs = s.workspace.recycle_begin_projection_for_test(s.cells, s.identity.fingerprint);
+    } else if (recycle == 3) {
+      s.workspace.recycle_clear_for_test();
+      rs = s.workspace.recycle_begin_initial_guess_guard_for_test(s.cells,
+                                                                  s.identity.fingerprint);
+    }
+    if (!rs) return code_of(rs);
+  }
   OwnedField b = make_field(44U, s.cells, 0U, 1U, 304U, 404U);
   OwnedField x = make_field(45U, s.cells, 1U, 1U, 305U, 405U);
   for (int k = 0; k < s.cells.z; ++k)
@@ -534,6 +558,11 @@ int hfref_solve(void* handle, const double* rhs, double* solution,
   outputs[7] = static_cast<double>(result.preconditioner_applies);
   outputs[8] = seconds;
   outputs[9] = s.setup_seconds;
+  outputs[10] = static_cast<double>(result.recycle_offered_directions);
+  outputs[11] = static_cast<double>(result.recycle_retained_directions);
+  outputs[12] = result.recycle_projection_accepted ? 1.0 : 0.0;
+  outputs[13] = result.recycle_projected_true_residual;
+  outputs[14] = static_cast<double>(result.recycle_cycle_corrections);
   return result.status ? 0 : code_of(result.status);
 }
 

@@ -39,7 +39,7 @@ def _load():
         lib.hfref_apply_operator.argtypes = [ctypes.c_void_p, dp, dp]
         lib.hfref_apply_mg.argtypes = [ctypes.c_void_p, dp, dp]
         lib.hfref_solve.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double, ctypes.c_double,
-                                    ctypes.c_int, ctypes.c_int, dp]
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         _lib = lib
     return _lib
 
@@ -139,13 +139,19 @@ class RefSession:
             raise RuntimeError(f"reference MG apply failed: {rc}")
         return z
 
+    RECYCLE = {"none": 0, "capture": 1, "project": 2, "guard": 3}
+
     def solve(self, rhs: np.ndarray, x0: Optional[np.ndarray] = None, rtol: float = 1e-10,
-              atol: float = 0.0, maxit: int = 400, true_residual_interval: int = 4):
+              atol: float = 0.0, maxit: int = 400, true_residual_interval: int = 4,
+              recycle: str = "none"):
+        """``recycle`` (FGMRES): "capture" opens a capture session (PISO corrector 1),
+        "project" projects its corrections (corrector 2), "guard" applies only the
+        zero-seed initial-guess guard, "none" clears any session."""
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         x = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64, order="C")
-        out = np.zeros(10)
+        out = np.zeros(15)
         rc = self._lib.hfref_solve(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
-                                   true_residual_interval, _dp(out))
+                                   true_residual_interval, self.RECYCLE[recycle], _dp(out))
         info = {
             "status": rc,
             "iterations": int(out[0]),
@@ -158,5 +164,10 @@ class RefSession:
             "preconditioner_applies": int(out[7]),
             "seconds": out[8],
             "setup_seconds": out[9],
+            "recycle_offered": int(out[10]),
+            "recycle_retained": int(out[11]),
+            "recycle_accepted": bool(out[12]),
+            "recycle_projected_residual": out[13],
+            "recycle_cycle_corrections": int(out[14]),
         }
         return x, info

@@ -94,6 +94,33 @@ def main():
             "fgmres_operator_applies": infof["operator_applies"],
         }
         print(name, index[name]["iterations_1e13"], index[name]["iterations_1e10"])
+    # Subspace recycling across two PISO correctors: corrector 1 captures its
+    # Arnoldi-cycle corrections, corrector 2 (warm-started, perturbed rhs)
+    # projects them (SolverWorkspace recycle_begin_capture /
+    # recycle_begin_projection, src/solver_linear_state.cpp:735-1037).
+    name = "sphere_24x20x16_prodF"
+    spec, pol = CASES[name]
+    system = system_for(spec)
+    rhs2 = workloads.warm_start_rhs(system, 1)
+    recycle = {}
+    arrays = {}
+    for restart in (12, 4):
+        ref = ref_oracle.RefSession(system, ref_oracle.MgPolicy(**pol), algorithm="fgmres",
+                                    restart=restart)
+        x1, i1 = ref.solve(system.rhs, rtol=1e-10, recycle="capture")
+        x2, i2 = ref.solve(rhs2, x0=x1, rtol=1e-10, recycle="project")
+        ref.close()
+        arrays[f"x1_r{restart}"], arrays[f"x2_r{restart}"] = x1, x2
+        recycle[str(restart)] = {
+            "capture_iterations": i1["iterations"],
+            "captured": i1["recycle_cycle_corrections"],
+            "project_iterations": i2["iterations"],
+            "offered": i2["recycle_offered"], "retained": i2["recycle_retained"],
+            "accepted": i2["recycle_accepted"],
+            "projected_residual": i2["recycle_projected_residual"],
+        }
+    np.savez_compressed(os.path.join(HERE, "recycle_sphere_24x20x16_prodF.npz"), **arrays)
+    index[name]["recycle"] = recycle
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(index, f, indent=1)
 

@@ -14,6 +14,7 @@ The C restatement (oracle/hfps_oracle.c) is pinned three ways:
   direct solve (tests/mpi/solver_krylov_mpi_test.cpp:1141-1193).
 """
 import dataclasses
+import os
 
 import numpy as np
 import pytest
@@ -85,6 +86,53 @@ def test_fgmres_short_restart_matches_live_reference():
                          restart=restart)
         assert (i1["iterations"], i1["operator_applies"]) == (i2["iterations"], i2["operator_applies"])
         assert np.array_equal(x1, x2)
+
+
+@pytest.mark.parametrize("restart", [12, 4])
+def test_recycling_restatement_reproduces_reference_golden(restart):
+    """Two PISO correctors: corrector 1 captures its Arnoldi-cycle
+    corrections, corrector 2 projects them before iterating
+    (src/solver_linear_state.cpp:735-1037; src/solver_krylov.cpp:1745-2019)."""
+    name = "sphere_24x20x16_prodF"
+    s = golden_cases.system(name)
+    meta = golden_cases.index()[name]["recycle"][str(restart)]
+    gold = np.load(os.path.join(golden_cases.GOLDEN, "recycle_sphere_24x20x16_prodF.npz"))
+    o = _oracle(s, golden_cases.policy(name), unit_linear=False)
+    x1, i1 = o.solve(s.rhs, rtol=1e-10, algorithm="fgmres", restart=restart, recycle="capture")
+    x2, i2 = o.solve(workloads.warm_start_rhs(s, 1), x0=x1, rtol=1e-10, algorithm="fgmres",
+                     restart=restart, recycle="project")
+    assert (i1["iterations"], i1["recycle_cycle_corrections"]) == (meta["capture_iterations"],
+                                                                   meta["captured"])
+    assert (i2["iterations"], i2["recycle_offered"], i2["recycle_retained"],
+            i2["recycle_accepted"]) == (meta["project_iterations"], meta["offered"],
+                                        meta["retained"], meta["accepted"])
+    assert i2["recycle_projected_residual"] == meta["projected_residual"]
+    assert np.array_equal(x1, gold[f"x1_r{restart}"])
+    assert np.array_equal(x2, gold[f"x2_r{restart}"])
+
+
+def test_recycling_short_restarts_and_guard_match_live_reference():
+    import ref_oracle
+    if not ref_oracle.available():
+        pytest.skip("compiled reference not built (make -C oracle ref)")
+    s = workloads.make("sphere64", n=(18, 14, 12), seed=8)
+    pol = ref_oracle.MgPolicy.production()
+    rhs2 = workloads.warm_start_rhs(s, 2)
+    for restart in (3, 2):
+        r = ref_oracle.RefSession(s, pol, algorithm="fgmres", restart=restart)
+        o = _oracle(s, pol, unit_linear=False)
+        kw = dict(algorithm="fgmres", restart=restart)
+        y1, _ = r.solve(s.rhs, rtol=1e-10, recycle="capture")
+        x1, _ = o.solve(s.rhs, rtol=1e-10, recycle="capture", **kw)
+        y2, j2 = r.solve(rhs2, x0=y1, rtol=1e-10, recycle="project")
+        x2, i2 = o.solve(rhs2, x0=x1, rtol=1e-10, recycle="project", **kw)
+        assert np.array_equal(x2, y2)
+        assert (i2["iterations"], i2["recycle_retained"]) == (j2["iterations"], j2["recycle_retained"])
+        # zero-seed guard: a wild initial guess is replaced by x0 = 0
+        y3, j3 = r.solve(rhs2, x0=50 * y1, rtol=1e-10, recycle="guard")
+        x3, i3 = o.solve(rhs2, x0=50 * x1, rtol=1e-10, recycle="guard", **kw)
+        assert j3["initial_true_residual"] == i3["initial_true_residual"] == j3["rhs_norm"]
+        assert np.array_equal(x3, y3)
 
 
 def test_restatement_matches_live_reference():
