@@ -74,6 +74,7 @@ void hfps_default_control(hfps_control* c) {
   c->restart = 0;
   c->algorithm = HFPS_PCG;
   c->precision = HFPS_FP64;
+  c->recycle = HFPS_RECYCLE_NONE;
 }
 
 int hfps_create(const hfps_geometry* geometry, const hfps_policy* policy,

@@ -597,6 +597,20 @@ __global__ void k_multidot(int n, BasisRefs basis, const double* __restrict__ w,
   }
 }
 
+__global__ void k_difference_nonzero(int n, const double* __restrict__ x,
+                                     double* __restrict__ snap, Scalars* scalars) {
+  grid_dependency_sync();
+  int nonzero = 0;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const double v = x[c] - snap[c];
+    nonzero |= v != 0.0;
+    snap[c] = v;
+  }
+  if (__any_sync(0xffffffffu, nonzero) && (threadIdx.x & 31) == 0)
+    atomicOr(&scalars->marks, 1u);
+}
+
 // out = scale * (dst + s_0 v_0 + s_1 v_1 + ...), terms added per cell in
 // basis order (add_scaled_basis, :510-564), then optionally scaled
 // (scale_copy, :611-625); `out` may be `dst`.
@@ -1243,6 +1257,10 @@ void launch_operator_shift(cudaStream_t s, const Level<double>& L, const double*
 void launch_multidot(cudaStream_t s, int n, const BasisRefs& basis, const double* w,
                      bool self, double* out, Reduce red) {
   launch(k_multidot, reduction_blocks(n), kThreads, 0, s, n, basis, w, self ? 1 : 0, out, red);
+}
+void launch_difference_nonzero(cudaStream_t s, int n, const double* x, double* snap,
+                               Scalars* scalars) {
+  launch(k_difference_nonzero, grid_for(n), kThreads, 0, s, n, x, snap, scalars);
 }
 void launch_basis_update(cudaStream_t s, int n, const double* dst, const BasisRefs& basis,
                          double scale, bool scaled, double* out) {

@@ -28,6 +28,7 @@ struct Scalars {
   double misc[4];
   double hcol[72];   // FGMRES: projections of the current column and |w|^2
   int flags;         // bit 0 non-finite, bit 1 breakdown, bit 2 invalid assembly input
+  unsigned marks;    // bit 0: a difference had a nonzero entry (recycle capture)
   unsigned counters[8];  // last-block arrival counters, one per reduction
 };
 
@@ -176,6 +177,10 @@ void launch_operator_shift(cudaStream_t s, const Level<double>& L, const double*
 // (count + self <= kBasisChunk); non-finite sums set flags bit 0.
 void launch_multidot(cudaStream_t s, int n, const BasisRefs& basis, const double* w,
                      bool self, double* out, Reduce red);
+// snap = x - snap; marks bit 0 when any entry is nonzero
+// (difference_recycle_field, src/solver_linear_state.cpp:162-181).
+void launch_difference_nonzero(cudaStream_t s, int n, const double* x, double* snap,
+                               Scalars* scalars);
 // out = (scaled ? scale : 1) * (dst + sum_r s_r v_r), per cell in basis order.
 void launch_basis_update(cudaStream_t s, int n, const double* dst, const BasisRefs& basis,
                          double scale, bool scaled, double* out);

@@ -123,6 +123,7 @@ Solver::~Solver() {
   if (h_scalars_ != nullptr) cudaFreeHost(h_scalars_);
   if (arena_ != nullptr) cudaFree(arena_);
   if (fg_storage_ != nullptr) cudaFree(fg_storage_);
+  if (rc_storage_ != nullptr) cudaFree(rc_storage_);
   if (own_stream_ && stream_ != nullptr) cudaStreamDestroy(stream_);
 }
 
@@ -945,6 +946,157 @@ Status Solver::ensure_fgmres_storage(uint32_t restart) {
   return {};
 }
 
+Status Solver::ensure_recycle_storage() {
+  if (rc_storage_ != nullptr) return {};
+  const size_t n = static_cast<size_t>(nx_) * ny_ * nz_;
+  const size_t stride = (n + 31) & ~static_cast<size_t>(31);
+  Status st = check(cudaMalloc(&rc_storage_, (2 * kRecycleMax + 1) * stride * sizeof(double)),
+                    "recycle storage");
+  if (!st) {
+    rc_storage_ = nullptr;
+    return st;
+  }
+  for (int i = 0; i < kRecycleMax; ++i) {
+    rc_ring_[i] = rc_storage_ + i * stride;
+    rc_image_[i] = rc_storage_ + (kRecycleMax + 1 + i) * stride;
+  }
+  rc_snapshot_ = rc_storage_ + kRecycleMax * stride;
+  return {};
+}
+
+// recycle_capture_cycle_publish (src/solver_linear_state.cpp:897-1017):
+// the cycle's correction x - snapshot enters the ring when it has a nonzero
+// entry, replacing the oldest of four.
+Status Solver::recycle_publish(const double* x, hfps_result& result) {
+  if (!rc_capture_ || !rc_cycle_active_) return {};
+  const int n = nx_ * ny_ * nz_;
+  Status st = check(cudaMemsetAsync(&d_scalars_->marks, 0, sizeof(unsigned), stream_),
+                    "recycle mark");
+  if (!st) return st;
+  launch_difference_nonzero(stream_, n, x, rc_snapshot_, d_scalars_);
+  launches_ += 1;
+  st = sync_scalars();
+  if (!st) return st;
+  rc_cycle_active_ = false;
+  if (!(h_scalars_->marks & 1u)) return {};
+  ++result.recycle_captured;
+  const int slot = rc_count_ < kRecycleMax ? (rc_oldest_ + rc_count_) % kRecycleMax : rc_oldest_;
+  std::swap(rc_ring_[slot], rc_snapshot_);
+  if (rc_count_ < kRecycleMax) ++rc_count_;
+  else rc_oldest_ = (rc_oldest_ + 1) % kRecycleMax;
+  return {};
+}
+
+// apply_recycle_projection (src/solver_krylov.cpp:1745-2019): images A d_i,
+// a rank test against 64 eps max |A d_i|, two classical Gram-Schmidt passes
+// over the retained images (the directions follow), normalisation,
+// alpha_i = image_i . r and the candidate x + sum alpha_i d_i, taken when its
+// true residual is below the current one.  The projection's operator
+// applies are not counted as the solve's (as in the reference).
+Status Solver::recycle_project(const hfps_control& control, double tol, hfps_result& result) {
+  rc_pending_ = false;
+  const int n = nx_ * ny_ * nz_;
+  (void)control;
+  const Level<double> A = l64_[0].view(neumann_);
+  const auto red = [&](int op) { return Reduce{d_scalars_, d_partials_, op}; };
+  const int offered = rc_count_;
+  result.recycle_offered = static_cast<uint32_t>(offered);
+  double* images[kRecycleMax];
+  double* dirs[kRecycleMax];
+  double pre[kRecycleMax];
+  double max_pre = 0.0;
+  Status st;
+  for (int i = 0; i < offered; ++i) {
+    dirs[i] = rc_ring_[(rc_oldest_ + i) % kRecycleMax];
+    images[i] = rc_image_[i];
+    launch_level_apply<double>(stream_, A, dirs[i], images[i]);
+    launch_norm2(stream_, n, images[i], red(kOpMisc));
+    launches_ += 2;
+    st = sync_scalars();
+    if (!st) return st;
+    pre[i] = std::sqrt(h_scalars_->misc[0]);
+    max_pre = std::max(max_pre, pre[i]);
+  }
+  rc_count_ = 0;
+  rc_oldest_ = 0;
+  int kept[kRecycleMax];
+  int retained = 0;
+  if (offered > 0 && max_pre > 0.0 && std::isfinite(max_pre)) {
+    const double threshold = 64.0 * std::numeric_limits<double>::epsilon() * max_pre;
+    for (int i = 0; i < offered; ++i) {
+      if (!(pre[i] > threshold)) continue;
+      double image_norm = pre[i];
+      if (retained != 0) {
+        for (int pass = 0; pass < 2; ++pass) {
+          BasisRefs refs{};
+          refs.count = retained;
+          for (int p = 0; p < retained; ++p) refs.v[p] = images[kept[p]];
+          // k_multidot reads w = images[i] against the retained images
+          launch_multidot(stream_, n, refs, images[i], false, d_scalars_->hcol,
+                          red(kCounterMultidot));
+          launches_ += 1;
+          st = sync_scalars();
+          if (!st) return st;
+          BasisRefs img{}, dir{};
+          img.count = dir.count = retained;
+          for (int p = 0; p < retained; ++p) {
+            img.v[p] = images[kept[p]];
+            dir.v[p] = dirs[kept[p]];
+            img.s[p] = dir.s[p] = -h_scalars_->hcol[p];
+          }
+          launch_basis_update(stream_, n, images[i], img, 1.0, false, images[i]);
+          launch_basis_update(stream_, n, dirs[i], dir, 1.0, false, dirs[i]);
+          launches_ += 2;
+        }
+        launch_norm2(stream_, n, images[i], red(kOpMisc));
+        launches_ += 1;
+        st = sync_scalars();
+        if (!st) return st;
+        image_norm = std::sqrt(h_scalars_->misc[0]);
+      }
+      if (!(image_norm > threshold) || !std::isfinite(image_norm)) continue;
+      BasisRefs none{};
+      launch_basis_update(stream_, n, images[i], none, 1.0 / image_norm, true, images[i]);
+      launch_basis_update(stream_, n, dirs[i], none, 1.0 / image_norm, true, dirs[i]);
+      launches_ += 2;
+      kept[retained++] = i;
+    }
+  }
+  result.recycle_retained = static_cast<uint32_t>(retained);
+  if (retained == 0) return {};
+  BasisRefs refs{};
+  refs.count = retained;
+  for (int p = 0; p < retained; ++p) refs.v[p] = images[kept[p]];
+  launch_multidot(stream_, n, refs, fg_v_[0], false, d_scalars_->hcol, red(kCounterMultidot));
+  launches_ += 1;
+  st = sync_scalars();
+  if (!st) return st;
+  BasisRefs dir{};
+  dir.count = retained;
+  for (int p = 0; p < retained; ++p) {
+    dir.v[p] = dirs[kept[p]];
+    dir.s[p] = h_scalars_->hcol[p];
+  }
+  double* candidate = rc_snapshot_;
+  launch_basis_update(stream_, n, kx_, dir, 1.0, false, candidate);
+  launch_residual_norm(stream_, A, candidate, kb_, fg_w_, red(kOpRecursive));
+  launches_ += 2;
+  st = sync_scalars();
+  if (!st) return st;
+  const double candidate_norm = std::sqrt(h_scalars_->rr);
+  result.recycle_projected_residual = candidate_norm;
+  if (std::isfinite(candidate_norm) && candidate_norm < result.final_true_residual) {
+    launch_copy(stream_, n, candidate, kx_);
+    launch_copy(stream_, n, fg_w_, fg_v_[0]);
+    launches_ += 2;
+    result.final_true_residual = candidate_norm;
+    result.recursive_residual = candidate_norm;
+    result.recycle_accepted = 1;
+  }
+  (void)tol;
+  return {};
+}
+
 // solve_fgmres (src/solver_krylov.cpp:1557-2650), same control flow: the
 // single-reduction Arnoldi step on w = A z_j - v_j (shift 1, :35) with one
 // batched reduction for the projections and |w|^2, the Pythagorean norm
@@ -967,6 +1119,27 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
   const auto red = [&](int op) { return Reduce{d_scalars_, d_partials_, op}; };
   Status st = ensure_fgmres_storage(restart);
   if (!st) return st;
+  // Recycle session as PressureVelocityCoupler selects it per corrector
+  // (src/solver_piso.cpp:10410-10433).
+  if (control.recycle != HFPS_RECYCLE_NONE) {
+    st = ensure_recycle_storage();
+    if (!st) return st;
+  }
+  const auto recycle_clear = [&]() {
+    rc_capture_ = rc_guard_only_ = rc_cycle_active_ = rc_pending_ = false;
+    rc_count_ = rc_oldest_ = 0;
+  };
+  switch (control.recycle) {
+    case HFPS_RECYCLE_CAPTURE: recycle_clear(); rc_capture_ = true; break;
+    case HFPS_RECYCLE_PROJECT:
+      if (!rc_capture_ || rc_cycle_active_ || rc_pending_)
+        return fail(HFPS_INVALID_PLAN, kDetailPlan, "projection without a capture session");
+      rc_capture_ = false;
+      rc_pending_ = true;
+      break;
+    case HFPS_RECYCLE_GUARD: recycle_clear(); rc_guard_only_ = true; break;
+    default: recycle_clear(); break;
+  }
   st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
   if (!st) return st;
   launch_norm2(stream_, n, kb_, red(kOpMisc));
@@ -1049,12 +1222,29 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
   double initial = 0.0;
   st = true_residual(kx_, V[0], initial);
   if (!st) return st;
+  // reset_to_zero_initial_guess under the recycle guard (:1673-1686).
+  if ((rc_capture_ || rc_guard_only_) && initial > bnorm) {
+    st = check(cudaMemsetAsync(kx_, 0, n * sizeof(double), stream_), "zero seed");
+    if (!st) return st;
+    launch_copy(stream_, n, kb_, V[0]);
+    launches_ += 1;
+    initial = bnorm;
+  }
   result.initial_true_residual = initial;
   result.final_true_residual = initial;
   result.recursive_residual = initial;
   if (initial <= tol) {
+    rc_pending_ = false;
     result.termination = HFPS_CONVERGED;
     return {};
+  }
+  if (rc_pending_) {
+    st = recycle_project(control, tol, result);
+    if (!st) return st;
+    if (result.recycle_accepted && result.final_true_residual <= tol) {
+      result.termination = HFPS_CONVERGED;
+      return {};
+    }
   }
   const size_t rows = restart + 1;
   std::vector<double> h(rows * restart, 0.0), cs(restart, 0.0), sn(restart, 0.0),
@@ -1087,6 +1277,12 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
     return {};
   };
   while (it < control.maximum_iterations) {
+    if (rc_capture_) {
+      // recycle_capture_cycle_start (src/solver_linear_state.cpp:857-895)
+      launch_copy(stream_, n, kx_, rc_snapshot_);
+      launches_ += 1;
+      rc_cycle_active_ = true;
+    }
     const double beta = result.final_true_residual;
     basis_update(V[0], nullptr, nullptr, 0, 1.0 / beta, true, V[0]);
     std::fill(g.begin(), g.end(), 0.0);
@@ -1127,6 +1323,8 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
         basis_update(kx_, Z.data(), y.data(), static_cast<int>(column), 1.0, false, kx_);
         double norm = 0.0;
         st = true_residual(kx_, V[0], norm);
+        if (!st) return st;
+        st = recycle_publish(kx_, result);
         if (!st) return st;
         result.final_true_residual = norm;
         record(norm);
@@ -1209,6 +1407,8 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
         if (!st) return st;
         result.final_true_residual = audited;
         if (audited <= tol) {
+          st = recycle_publish(trial, result);
+          if (!st) return st;
           launch_copy(stream_, n, trial, kx_);
           launches_ += 1;
           result.termination = HFPS_CONVERGED;
@@ -1219,6 +1419,8 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
       basis_update(kx_, Z.data(), y.data(), count, 1.0, false, kx_);
       double norm = 0.0;
       st = true_residual(kx_, V[0], norm);
+      if (!st) return st;
+      st = recycle_publish(kx_, result);
       if (!st) return st;
       result.final_true_residual = norm;
       result.recursive_residual = norm;
@@ -1259,6 +1461,8 @@ Status Solver::solve(const double* rhs, double* solution, int memory,
       control.relative_tolerance < 0.0 || control.absolute_tolerance < 0.0 ||
       (control.relative_tolerance == 0.0 && control.absolute_tolerance == 0.0) ||
       (control.precision != HFPS_FP64 && control.precision != HFPS_MIXED) ||
+      control.recycle < HFPS_RECYCLE_NONE || control.recycle > HFPS_RECYCLE_GUARD ||
+      (control.algorithm == HFPS_PCG && control.recycle != HFPS_RECYCLE_NONE) ||
       !((control.algorithm == HFPS_PCG && control.restart == 0 && policy_.unit_linear) ||
         (control.algorithm == HFPS_FGMRES && control.restart >= 1 &&
          control.restart <= static_cast<uint32_t>(kMaxFgmresRestart))))

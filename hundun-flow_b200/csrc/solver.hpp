@@ -109,6 +109,9 @@ class Solver {
   Status krylov_fgmres(const hfps_control& control, hfps_result& result,
                        double* history, uint32_t capacity);
   Status ensure_fgmres_storage(uint32_t restart);
+  Status ensure_recycle_storage();
+  Status recycle_publish(const double* x, hfps_result& result);
+  Status recycle_project(const hfps_control& control, double tol, hfps_result& result);
   Status sync_scalars();
   Status copy_in(double* dst, const double* src, size_t n, int memory);
   Status copy_out(double* dst, const double* src, size_t n, int memory);
@@ -161,6 +164,18 @@ class Solver {
   std::vector<double*> fg_v_;
   std::vector<double*> fg_z_;
   double* fg_w_{};
+  // FGMRES subspace recycling across solves (hfps_recycle): a ring of up to
+  // four cycle corrections (oldest first from rc_oldest_) and the snapshot
+  // of x at the current cycle's start.  Publishing swaps the snapshot buffer
+  // into the ring instead of copying it.  The projection's images A d_i use
+  // four scratch vectors of their own.
+  static constexpr int kRecycleMax = 4;
+  double* rc_storage_{};
+  double* rc_ring_[kRecycleMax]{};
+  double* rc_snapshot_{};
+  double* rc_image_[kRecycleMax]{};   // projection scratch: A d_i
+  bool rc_capture_{}, rc_guard_only_{}, rc_cycle_active_{}, rc_pending_{};
+  int rc_count_{}, rc_oldest_{};
   cudaGraphExec_t mg_graph_[2]{};
   size_t mg_nodes_[2]{};      // kernels per MG application (graph nodes)
   uint64_t launches_{};       // kernels launched since the last reset

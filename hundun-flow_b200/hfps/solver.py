@@ -25,6 +25,7 @@ LIBRARY = os.path.join(PACKAGE, "libhfps.so")
 HOST, DEVICE = 0, 1
 FP64, MIXED = 0, 1
 PCG, FGMRES = 0, 1
+RECYCLE = {"none": 0, "capture": 1, "project": 2, "guard": 3}
 
 STATUS = ["ok", "invalid_case", "invalid_plan", "allocation_failure", "mpi_failure",
           "numerical_failure", "rejected_step", "io_failure"]
@@ -88,7 +89,7 @@ class Control(ctypes.Structure):
                 ("maximum_iterations", ctypes.c_uint32),
                 ("true_residual_interval", ctypes.c_uint32),
                 ("restart", ctypes.c_uint32), ("algorithm", ctypes.c_int),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("recycle", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -101,7 +102,10 @@ class Result(ctypes.Structure):
                 ("operator_applies", ctypes.c_uint64),
                 ("preconditioner_applies", ctypes.c_uint64),
                 ("history_length", ctypes.c_uint32), ("levels", ctypes.c_uint32),
-                ("seconds", ctypes.c_double), ("kernel_launches", ctypes.c_uint64)]
+                ("seconds", ctypes.c_double), ("kernel_launches", ctypes.c_uint64),
+                ("recycle_offered", ctypes.c_uint32), ("recycle_retained", ctypes.c_uint32),
+                ("recycle_accepted", ctypes.c_uint32), ("recycle_captured", ctypes.c_uint32),
+                ("recycle_projected_residual", ctypes.c_double)]
 
     def as_dict(self):
         d = {name: getattr(self, name) for name, _ in self._fields_}
@@ -222,6 +226,7 @@ class SolveOptions:
     precision: int = FP64
     algorithm: int = PCG   # PCG (solve_pcg) or FGMRES (solve_fgmres)
     restart: int = 0       # FGMRES restart length (the reference's default is 12)
+    recycle: str = "none"  # FGMRES: "none", "capture", "project", "guard"
 
 
 class PressureSolver:
@@ -404,6 +409,7 @@ class PressureSolver:
         c.restart = options.restart if options.algorithm == FGMRES else 0
         if options.algorithm == FGMRES and c.restart == 0:
             c.restart = 12
+        c.recycle = RECYCLE[options.recycle]
         return c
 
     def solve(self, rhs, x0=None, options: Optional[SolveOptions] = None, out=None,

@@ -114,7 +114,23 @@ typedef struct hfps_control {
   uint32_t restart;   /* FGMRES restart length; 0 for PCG */
   int algorithm;      /* hfps_algorithm */
   int precision;      /* hfps_precision */
+  int recycle;        /* hfps_recycle (FGMRES only) */
 } hfps_control;
+
+/* Subspace recycling across consecutive pressure solves (FGMRES only), as
+ * PressureVelocityCoupler selects it per corrector (src/solver_piso.cpp:
+ * 10410-10433; SolverWorkspace recycle state, src/solver_linear_state.cpp:
+ * 735-1037).  CAPTURE (corrector 1) records the correction of every Arnoldi
+ * cycle, up to the 4 latest; PROJECT (corrector 2, same system) starts from
+ * the least-squares combination of them when that lowers the true residual
+ * (src/solver_krylov.cpp:1745-2019); GUARD only replaces an initial guess
+ * whose residual exceeds |b| by zero (also active while capturing). */
+typedef enum hfps_recycle {
+  HFPS_RECYCLE_NONE = 0,
+  HFPS_RECYCLE_CAPTURE = 1,
+  HFPS_RECYCLE_PROJECT = 2,
+  HFPS_RECYCLE_GUARD = 3
+} hfps_recycle;
 
 /* LinearSolveResult subset (include/hundun/v04_linear.hpp:530-579). */
 typedef struct hfps_result {
@@ -133,6 +149,11 @@ typedef struct hfps_result {
   uint32_t levels;           /* MG levels in the hierarchy */
   double seconds;            /* wall time of the solve on the host */
   uint64_t kernel_launches;  /* this library's kernels launched by the call */
+  uint32_t recycle_offered;      /* captured corrections offered to the projection */
+  uint32_t recycle_retained;     /* kept after the rank test */
+  uint32_t recycle_accepted;     /* 1 when the projected start was taken */
+  uint32_t recycle_captured;     /* corrections captured by this solve */
+  double recycle_projected_residual;
 } hfps_result;
 
 typedef struct hfps_solver hfps_solver;

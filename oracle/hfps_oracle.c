@@ -60,6 +60,7 @@ typedef struct {
   int rc_count, rc_oldest;
   double* rc_ring[4];
   double* rc_snapshot;
+  double* rc_image[4]; /* projection scratch: A d_i */
 } oracle_t;
 
 static size_t idx(const int* n, int i, int j, int k) {
@@ -972,7 +973,10 @@ int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
   double rc_projected = 0.0;
   if (o->rc_snapshot == NULL) {
     o->rc_snapshot = calloc(n, sizeof(double));
-    for (int r = 0; r < RECYCLE_MAX; ++r) o->rc_ring[r] = calloc(n, sizeof(double));
+    for (int r = 0; r < RECYCLE_MAX; ++r) {
+      o->rc_ring[r] = calloc(n, sizeof(double));
+      o->rc_image[r] = calloc(n, sizeof(double));
+    }
   }
   /* Session selection as PressureVelocityCoupler makes it
    * (src/solver_piso.cpp:10410-10433). */
@@ -1048,9 +1052,7 @@ int hfo_solve_fgmres(void* handle, const double* rhs, double* x, double rtol,
     double max_pre = 0.0;
     for (int i = 0; i < offered; ++i) {
       dirs[i] = recycle_slot(o, i);
-      /* workspace slot v_begin + 1 + i: basis slots, then the (still free)
-       * preconditioned-basis slots when the restart is short */
-      images[i] = 1 + i < rows ? V[1 + i] : Z[1 + i - rows];
+      images[i] = o->rc_image[i];
       hfo_apply_operator(o, dirs[i], images[i]);
       pre[i] = norm2(images[i], n, &ok);
       if (pre[i] > max_pre) max_pre = pre[i];
@@ -1332,7 +1334,7 @@ void hfo_destroy(void* handle) {
   }
   for (int a = 0; a < 3; ++a) free(o->faces[a]);
   for (int w = 0; w < 6; ++w) free(o->work[w]);
-  for (int r = 0; r < 4; ++r) free(o->rc_ring[r]);
+  for (int r = 0; r < 4; ++r) { free(o->rc_ring[r]); free(o->rc_image[r]); }
   free(o->rc_snapshot);
   free(o->diag0); free(o->fx0); free(o->fy0); free(o->fz0); free(o->active);
   free(o);

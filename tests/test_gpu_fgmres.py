@@ -137,3 +137,56 @@ def test_pcg_needs_unit_scaling(hfps_mod):
     with pytest.raises(hfps_mod.SolverError) as err:
         g.solve(s.rhs)
     assert err.value.status == 2
+
+
+@pytest.mark.parametrize("restart", [12, 4, 1])
+def test_recycling_across_correctors_matches_restatement(hfps_mod, restart):
+    """Corrector 1 captures its cycle corrections, corrector 2 projects them
+    (SolverWorkspace recycle state, src/solver_linear_state.cpp:735-1037;
+    apply_recycle_projection, src/solver_krylov.cpp:1745-2019)."""
+    name = "sphere_24x20x16_prodF"
+    s = golden_cases.system(name)
+    pol = golden_cases.policy(name)
+    g = hfps_mod.PressureSolver.from_system(s, gpu_policy(hfps_mod, pol))
+    o = oracle(s, pol)
+    rhs2 = workloads.warm_start_rhs(s, 1)
+    kw = dict(rtol=1e-10, algorithm=hfps_mod.FGMRES, restart=restart)
+    x1, i1 = g.solve(s.rhs, recycle="capture", **kw)
+    x2, i2 = g.solve(rhs2, x0=x1, recycle="project", **kw)
+    okw = dict(rtol=1e-10, algorithm="fgmres", restart=restart)
+    y1, j1 = o.solve(s.rhs, recycle="capture", **okw)
+    y2, j2 = o.solve(rhs2, x0=y1, recycle="project", **okw)
+    assert i1["recycle_captured"] == j1["recycle_cycle_corrections"]
+    assert (i2["recycle_offered"], i2["recycle_retained"], bool(i2["recycle_accepted"])) == (
+        j2["recycle_offered"], j2["recycle_retained"], j2["recycle_accepted"])
+    assert i1["iterations"] == j1["iterations"]
+    if restart == 1:
+        # Single-step corrections are nearly dependent: the Gram-Schmidt
+        # amplifies the summation-order difference (compensated sums in the
+        # reference, fixed-order trees here) to ~1e-8 in the projected
+        # residual; both solves still converge to the tolerance.
+        assert abs(i2["recycle_projected_residual"] - j2["recycle_projected_residual"]) <= \
+            1e-6 * j2["recycle_projected_residual"]
+        assert abs(i2["iterations"] - j2["iterations"]) <= 1
+        assert np.linalg.norm(x2 - y2) / np.linalg.norm(y2) <= 1e-8
+        return
+    assert abs(i2["recycle_projected_residual"] - j2["recycle_projected_residual"]) <= \
+        1e-9 * j2["recycle_projected_residual"]
+    assert i2["iterations"] == j2["iterations"]
+    assert np.linalg.norm(x2 - y2) / np.linalg.norm(y2) <= 1e-12
+    meta = golden_cases.index()[name]["recycle"][str(restart)]
+    gold = np.load(golden_cases.GOLDEN + "/recycle_sphere_24x20x16_prodF.npz")
+    assert i2["iterations"] == meta["project_iterations"]
+    assert np.linalg.norm(x2 - gold[f"x2_r{restart}"]) / np.linalg.norm(x2) <= 1e-9
+
+
+def test_recycling_guard_and_session_rules(hfps_mod):
+    s = workloads.make("sphere64", n=(16, 14, 12), seed=4)
+    g = hfps_mod.PressureSolver.from_system(s, hfps_mod.Policy.production().replace(unit_linear=0))
+    kw = dict(rtol=1e-10, algorithm=hfps_mod.FGMRES, restart=12)
+    with pytest.raises(hfps_mod.SolverError) as err:
+        g.solve(s.rhs, recycle="project", **kw)        # no capture session
+    assert err.value.status == 2
+    x, info = g.solve(s.rhs, x0=np.full_like(s.rhs, 1e3), recycle="guard", **kw)
+    assert info["initial_true_residual"] == info["rhs_norm"]   # zero seed taken
+    assert info["termination"] == "converged"
