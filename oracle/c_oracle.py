@@ -44,6 +44,10 @@ def _load():
         lib.hfo_apply_mg.argtypes = [ctypes.c_void_p, dp, dp]
         lib.hfo_solve.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double, ctypes.c_double,
                                   ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int]
+        lib.hfo_apply_preconditioner.argtypes = [ctypes.c_void_p, dp, dp]
+        lib.hfo_solve_bicgstab.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp,
+                                           ctypes.c_int]
         lib.hfo_solve_fgmres.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                          ctypes.c_int, ctypes.c_int, dp, dp, ctypes.c_int]
@@ -66,7 +70,10 @@ class OracleSession:
     Gauss-Seidel, 1 the zebra order of the CUDA path.
     """
 
-    def __init__(self, system, policy=None, unit_linear: bool = True, line_order: int = 0):
+    PRECONDITIONERS = {"mg": 0, "dic": 1}
+
+    def __init__(self, system, policy=None, unit_linear: bool = True, line_order: int = 0,
+                 preconditioner: str = "mg"):
         from ref_oracle import MgPolicy  # same policy record as the reference driver
         policy = policy or MgPolicy()
         lib = _load()
@@ -74,9 +81,10 @@ class OracleSession:
         self.system = system
         self._faces = [np.ascontiguousarray(f, dtype=np.float64) for f in system.faces]
         bc = (ctypes.c_int * 6)(*system.boundary)
-        options = (ctypes.c_int * 11)(0, 0, policy.smoother, policy.cycle, policy.pre, policy.post,
+        options = (ctypes.c_int * 12)(0, 0, policy.smoother, policy.cycle, policy.pre, policy.post,
                                       policy.coarse_sweeps, 1 if unit_linear else 0,
-                                      policy.max_levels, policy.min_coarse_extent, line_order)
+                                      policy.max_levels, policy.min_coarse_extent, line_order,
+                                      self.PRECONDITIONERS[preconditioner])
         reals = (ctypes.c_double * 3)(policy.chebyshev_fraction, policy.anisotropy_threshold,
                                       policy.diagonal_shortcut)
         active = None
@@ -128,6 +136,14 @@ class OracleSession:
         self._lib.hfo_apply_level(self._handle, level, _dp(x), _dp(y))
         return y
 
+    def apply_preconditioner(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty_like(r)
+        rc = self._lib.hfo_apply_preconditioner(self._handle, _dp(r), _dp(z))
+        if rc != 0:
+            raise RuntimeError(f"oracle preconditioner failed: {rc}")
+        return z
+
     def apply_mg(self, r):
         r = np.ascontiguousarray(r, dtype=np.float64)
         z = np.empty_like(r)
@@ -146,7 +162,10 @@ class OracleSession:
         x = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64, order="C")
         out = np.zeros(13)
         hist = np.zeros(maxit)
-        if algorithm == "fgmres":
+        if algorithm == "bicgstab":
+            rc = self._lib.hfo_solve_bicgstab(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
+                                              true_residual_interval, _dp(out), _dp(hist), maxit)
+        elif algorithm == "fgmres":
             modes = {"none": 0, "capture": 1, "project": 2, "guard": 3}
             rc = self._lib.hfo_solve_fgmres(self._handle, _dp(rhs), _dp(x), rtol, atol, maxit,
                                             true_residual_interval, restart, modes[recycle],

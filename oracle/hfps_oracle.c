@@ -61,6 +61,14 @@ typedef struct {
   double* rc_ring[4];
   double* rc_snapshot;
   double* rc_image[4]; /* projection scratch: A d_i */
+  /* Cold-path preconditioner (ColdPressureIccg / ColdPressureDilu,
+   * src/solver_iccg.hpp:224-293, src/solver_cold.hpp:484-560): 0 the MG
+   * plan, 1 diagonal IC(0) in the reference's lexicographic order (the two
+   * classes coincide on the symmetric pressure rows). */
+  int pc_kind;
+  double* dic_diag;   /* decorated row diagonal */
+  double* dic_nb;     /* 6 couplings per row: x-, x+, y-, y+, z-, z+ */
+  double* dic_inv;    /* inverse pivots */
 } oracle_t;
 
 static size_t idx(const int* n, int i, int j, int k) {
@@ -708,6 +716,104 @@ int hfo_apply_mg(void* handle, const double* residual, double* correction) {
 }
 
 /* ------------------------------------------------------------------ */
+/* Cold-path diagonal incomplete Cholesky (DIC / IC(0))                 */
+/* ------------------------------------------------------------------ */
+/* Rows of the IBM-decorated operator: identity rows on solid cells; a link
+ * to a solid cell or a Neumann boundary face leaves the row's couplings and
+ * its coefficient leaves the diagonal (subtracted in face order). */
+static void dic_rows(oracle_t* o) {
+  const int* n = o->n;
+  const size_t cells = o->lv[0].cells;
+  for (int k = 0; k < n[2]; ++k)
+    for (int j = 0; j < n[1]; ++j)
+      for (int i = 0; i < n[0]; ++i) {
+        const size_t c = idx(n, i, j, k);
+        double* nb = o->dic_nb + 6 * c;
+        for (int f = 0; f < 6; ++f) nb[f] = 0.0;
+        if (!cell_active(o, i, j, k)) { o->dic_diag[c] = 1.0; continue; }
+        double d = o->diag0[c];
+        const double face[6] = {o->fx0[fidx_x(n, i, j, k)], o->fx0[fidx_x(n, i + 1, j, k)],
+                                o->fy0[fidx_y(n, i, j, k)], o->fy0[fidx_y(n, i, j + 1, k)],
+                                o->fz0[fidx_z(n, i, j, k)], o->fz0[fidx_z(n, i, j, k + 1)]};
+        const int at[3] = {i, j, k};
+        for (int f = 0; f < 6; ++f) {
+          const int a = f / 2;
+          int q[3] = {i, j, k};
+          q[a] += (f & 1) ? 1 : -1;
+          if (q[a] < 0 || q[a] >= n[a]) {
+            if (o->bc[f] == BC_NEUMANN) d -= face[f];
+            continue;
+          }
+          if (!cell_active(o, q[0], q[1], q[2])) { d -= face[f]; continue; }
+          nb[f] = face[f];
+          (void)at;
+        }
+        o->dic_diag[c] = d;
+      }
+  (void)cells;
+}
+
+/* ColdPressureIccg::prepare (src/solver_iccg.hpp:236-256): lexicographic
+ * pivots p_i = D_i - sum_axis c^2 / p_(lower neighbour). */
+static int dic_prepare(oracle_t* o) {
+  const int* n = o->n;
+  const size_t stride[3] = {1, (size_t)n[0], (size_t)n[0] * n[1]};
+  size_t i = 0;
+  for (int z = 0; z < n[2]; ++z)
+    for (int y = 0; y < n[1]; ++y)
+      for (int x = 0; x < n[0]; ++x, ++i) {
+        const int at[3] = {x, y, z};
+        double pivot = o->dic_diag[i];
+        for (int a = 0; a < 3; ++a) {
+          const double lower = o->dic_nb[6 * i + 2 * a];
+          if (at[a] > 0) pivot -= lower * lower * o->dic_inv[i - stride[a]];
+        }
+        if (!(pivot > 0) || !isfinite(pivot)) return 5;
+        o->dic_inv[i] = 1 / pivot;
+      }
+  return 0;
+}
+
+/* ColdPressureIccg::apply (src/solver_iccg.hpp:262-284): forward sweep with
+ * the lower couplings, backward sweep with the upper ones (the next cell's
+ * lower coupling). */
+static void dic_apply(const oracle_t* o, const double* in, double* out) {
+  const int* n = o->n;
+  const size_t sy = (size_t)n[0], sz = sy * n[1];
+  size_t i = 0;
+  for (int z = 0; z < n[2]; ++z)
+    for (int y = 0; y < n[1]; ++y)
+      for (int x = 0; x < n[0]; ++x, ++i) {
+        double value = in[i];
+        if (x > 0) value += o->dic_nb[6 * i + 0] * out[i - 1];
+        if (y > 0) value += o->dic_nb[6 * i + 2] * out[i - sy];
+        if (z > 0) value += o->dic_nb[6 * i + 4] * out[i - sz];
+        out[i] = value * o->dic_inv[i];
+      }
+  i = o->lv[0].cells;
+  for (int z = n[2] - 1; z >= 0; --z)
+    for (int y = n[1] - 1; y >= 0; --y)
+      for (int x = n[0] - 1; x >= 0; --x) {
+        --i;
+        double value = 0;
+        if (x + 1 < n[0]) value += o->dic_nb[6 * (i + 1) + 0] * out[i + 1];
+        if (y + 1 < n[1]) value += o->dic_nb[6 * (i + sy) + 2] * out[i + sy];
+        if (z + 1 < n[2]) value += o->dic_nb[6 * (i + sz) + 4] * out[i + sz];
+        out[i] += value * o->dic_inv[i];
+      }
+}
+
+static int apply_pc(oracle_t* o, const double* r, double* z) {
+  if (o->pc_kind == 0) return hfo_apply_mg(o, r, z);
+  dic_apply(o, r, z);
+  return 0;
+}
+
+int hfo_apply_preconditioner(void* handle, const double* r, double* z) {
+  return apply_pc(handle, r, z);
+}
+
+/* ------------------------------------------------------------------ */
 /* Exact operator: regular stencil + IBM decoration                    */
 /* (src/solver_pressure.cpp:746-811; src/solver_ibm_pressure.cpp:347-385)*/
 /* ------------------------------------------------------------------ */
@@ -837,7 +943,7 @@ int hfo_solve(void* handle, const double* rhs, double* x, double rtol,
   int term = TERM_MAXIMUM;
   int status = 6;
   if (initial <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
-  hfo_apply_mg(o, r, z);
+  apply_pc(o, r, z);
   ++pc_applies;
   double rho = dot(r, z, n, &ok);
   if (!(rho > 0.0) || !isfinite(rho)) { term = TERM_BREAKDOWN; status = 5; goto done; }
@@ -858,14 +964,14 @@ int hfo_solve(void* handle, const double* rhs, double* x, double rtol,
       TRUE_RESIDUAL(final_true);
       if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
       if (it == maxit) { term = TERM_MAXIMUM; status = 6; goto done; }
-      hfo_apply_mg(o, r, z);
+      apply_pc(o, r, z);
       ++pc_applies;
       rho = dot(r, z, n, &ok);
       if (!(rho > 0.0) || !isfinite(rho)) { term = TERM_BREAKDOWN; status = 5; goto done; }
       memcpy(p, z, n * sizeof(double));
       continue;
     }
-    hfo_apply_mg(o, r, z);
+    apply_pc(o, r, z);
     ++pc_applies;
     const double rho_next = dot(r, z, n, &ok);
     if (!(rho_next > 0.0) || !isfinite(rho_next)) { term = TERM_BREAKDOWN; status = 5; goto done; }
@@ -1267,6 +1373,124 @@ done:
 }
 
 /* ------------------------------------------------------------------ */
+/* solve_bicgstab (src/solver_krylov.cpp:2651-3090) with the default      */
+/* control (no bounded recurrence, no maximum norm, no best-iterate        */
+/* retention): early exit on |s|, restart after every true-residual        */
+/* verification that does not converge, rho carried from the fused update. */
+/* ------------------------------------------------------------------ */
+int hfo_solve_bicgstab(void* handle, const double* rhs, double* x, double rtol,
+                       double atol, int maxit, int tri, double* out, double* history,
+                       int hcap) {
+  oracle_t* o = handle;
+  const size_t n = o->lv[0].cells;
+  int ok = 1, it = 0, term = TERM_MAXIMUM, status = 6;
+  long op_applies = 0, pc_applies = 0;
+  memset(out, 0, 8 * sizeof(double));
+  double* r = malloc(n * sizeof(double));
+  double* rh = malloc(n * sizeof(double));
+  double* p = malloc(n * sizeof(double));
+  double* sv = malloc(n * sizeof(double));
+  double* ph = malloc(n * sizeof(double));
+  double* sh = malloc(n * sizeof(double));
+  double* v = malloc(n * sizeof(double));
+  double* t = malloc(n * sizeof(double));
+  double* ax = malloc(n * sizeof(double));
+  double initial = 0.0, final_true = 0.0;
+  const double bnorm = norm2(rhs, n, &ok);
+  if (!ok) { term = TERM_NON_FINITE; status = 5; goto done; }
+  const double tol = atol > rtol * bnorm ? atol : rtol * bnorm;
+  out[4] = bnorm;
+  out[5] = tol;
+  if (bnorm == 0.0) { memset(x, 0, n * sizeof(double)); term = TERM_ZERO_RHS; status = 0; goto done; }
+#define TRUE_RESIDUAL(dst_norm)                                           \
+  do {                                                                    \
+    hfo_apply_operator(o, x, ax);                                         \
+    ++op_applies;                                                         \
+    for (size_t c = 0; c < n; ++c) r[c] = 1.0 * rhs[c] + -1.0 * ax[c];    \
+    dst_norm = norm2(r, n, &ok);                                          \
+  } while (0)
+  TRUE_RESIDUAL(initial);
+  final_true = initial;
+  if (initial <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+  memcpy(rh, r, n * sizeof(double));
+  double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+  int fresh = 1;
+  while (it < maxit) {
+    const double rho = dot(rh, r, n, &ok);
+    if (rho == 0.0 || !isfinite(rho)) { term = TERM_BREAKDOWN; status = 5; goto done; }
+    if (fresh) {
+      memcpy(p, r, n * sizeof(double));
+    } else {
+      if (omega == 0.0 || !isfinite(omega)) { term = TERM_BREAKDOWN; status = 5; goto done; }
+      const double beta = (rho / rho_prev) * (alpha / omega);
+      for (size_t c = 0; c < n; ++c) {
+        const double intermediate = 1.0 * p[c] + -omega * v[c];
+        p[c] = 1.0 * r[c] + beta * intermediate;
+      }
+    }
+    apply_pc(o, p, ph);
+    ++pc_applies;
+    hfo_apply_operator(o, ph, v);
+    ++op_applies;
+    const double denominator = dot(rh, v, n, &ok);
+    if (denominator == 0.0 || !isfinite(denominator)) { term = TERM_BREAKDOWN; status = 5; goto done; }
+    alpha = rho / denominator;
+    for (size_t c = 0; c < n; ++c) sv[c] = 1.0 * r[c] + -alpha * v[c];
+    const double s_norm = norm2(sv, n, &ok);
+    if (s_norm <= tol) {
+      for (size_t c = 0; c < n; ++c) x[c] = x[c] + alpha * ph[c];
+      ++it;
+      TRUE_RESIDUAL(final_true);
+      if (history && it - 1 < hcap) history[it - 1] = final_true;
+      if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+      if (it == maxit) { term = TERM_MAXIMUM; status = 6; goto done; }
+      memcpy(rh, r, n * sizeof(double));
+      rho_prev = 1.0; alpha = 1.0; omega = 1.0; fresh = 1;
+      continue;
+    }
+    apply_pc(o, sv, sh);
+    ++pc_applies;
+    hfo_apply_operator(o, sh, t);
+    ++op_applies;
+    /* local_dot_pair(t, s): t.s and t.t, Neumaier each */
+    const double ts = dot(t, sv, n, &ok);
+    const double tt = dot(t, t, n, &ok);
+    if (!(tt > 0.0) || !isfinite(ts) || !isfinite(tt)) { term = TERM_BREAKDOWN; status = 5; goto done; }
+    omega = ts / tt;
+    if (omega == 0.0 || !isfinite(omega)) { term = TERM_BREAKDOWN; status = 5; goto done; }
+    for (size_t c = 0; c < n; ++c) {
+      const double intermediate = x[c] + alpha * ph[c];
+      x[c] = intermediate + omega * sh[c];
+      r[c] = 1.0 * sv[c] + -omega * t[c];
+    }
+    ++it;
+    const double recursive = norm2(r, n, &ok);
+    if (history && it - 1 < hcap) history[it - 1] = recursive;
+    const int verify = recursive <= tol || it % tri == 0 || it == maxit;
+    if (verify) {
+      TRUE_RESIDUAL(final_true);
+      if (final_true <= tol) { term = TERM_CONVERGED; status = 0; goto done; }
+      if (it == maxit) { term = TERM_MAXIMUM; status = 6; goto done; }
+      memcpy(rh, r, n * sizeof(double));
+      rho_prev = 1.0; alpha = 1.0; omega = 1.0; fresh = 1;
+      continue;
+    }
+    rho_prev = rho;
+    fresh = 0;
+  }
+done:
+#undef TRUE_RESIDUAL
+  out[0] = it;
+  out[1] = initial;
+  out[2] = final_true;
+  out[3] = term;
+  out[6] = (double)op_applies;
+  out[7] = (double)pc_applies;
+  free(r); free(rh); free(p); free(sv); free(ph); free(sh); free(v); free(t); free(ax);
+  return ok ? status : 5;
+}
+
+/* ------------------------------------------------------------------ */
 void* hfo_create(int nx, int ny, int nz, const double* xf, const double* yf,
                  const double* zf, const int* bc, const double* diagonal,
                  const double* fx, const double* fy, const double* fz,
@@ -1311,6 +1535,7 @@ void* hfo_create(int nx, int ny, int nz, const double* xf, const double* yf,
   o->max_levels = options[8];
   o->min_extent = options[9];
   o->line_order = options[10];
+  o->pc_kind = options[11];
   o->cheb_fraction = reals[0];
   o->anisotropy = reals[1];
   o->shortcut_ratio = reals[2];
@@ -1320,6 +1545,17 @@ void* hfo_create(int nx, int ny, int nz, const double* xf, const double* yf,
     return NULL;
   }
   select_shortcut(o);
+  if (o->pc_kind != 0) {
+    o->dic_diag = calloc(cells, sizeof(double));
+    o->dic_nb = calloc(6 * cells, sizeof(double));
+    o->dic_inv = calloc(cells, sizeof(double));
+    dic_rows(o);
+    if (dic_prepare(o) != 0) {
+      hfo_destroy(o);
+      *status = 5;
+      return NULL;
+    }
+  }
   *status = 0;
   return o;
 }
@@ -1335,6 +1571,7 @@ void hfo_destroy(void* handle) {
   for (int a = 0; a < 3; ++a) free(o->faces[a]);
   for (int w = 0; w < 6; ++w) free(o->work[w]);
   for (int r = 0; r < 4; ++r) { free(o->rc_ring[r]); free(o->rc_image[r]); }
+  free(o->dic_diag); free(o->dic_nb); free(o->dic_inv);
   free(o->rc_snapshot);
   free(o->diag0); free(o->fx0); free(o->fy0); free(o->fz0); free(o->active);
   free(o);

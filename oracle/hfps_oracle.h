@@ -21,7 +21,10 @@ extern "C" {
 /* options: [algorithm(0 pcg), restart, smoother(0 red-black,1 chebyshev),
  *           cycle(0 V,1 F), pre, post, coarse_sweeps, scaling(0 residual-
  *           minimising,1 unit_linear), max_levels, min_coarse_extent,
- *           line_order(0 lexicographic as the reference, 1 zebra)]
+ *           line_order(0 lexicographic as the reference, 1 zebra),
+ *           preconditioner(0 MG plan, 1 diagonal IC(0) in the reference's
+ *           lexicographic order = ColdPressureIccg / ColdPressureDilu on
+ *           symmetric rows)]
  * reals:   [chebyshev_fraction, anisotropy_threshold, diagonal_shortcut] */
 void* hfo_create(int nx, int ny, int nz, const double* x_faces,
                  const double* y_faces, const double* z_faces,
@@ -47,6 +50,14 @@ int hfo_solve(void* handle, const double* rhs, double* x,
               int maximum_iterations, int true_residual_interval,
               double* outputs, double* history, int history_capacity);
 
+/* z = M r with the session's preconditioner (MG plan or cold-path DIC). */
+int hfo_apply_preconditioner(void* handle, const double* r, double* z);
+/* solve_bicgstab (src/solver_krylov.cpp:2651-3090), default control; same
+ * outputs and history as hfo_solve. */
+int hfo_solve_bicgstab(void* handle, const double* rhs, double* x,
+                       double relative_tolerance, double absolute_tolerance,
+                       int maximum_iterations, int true_residual_interval,
+                       double* outputs, double* history, int history_capacity);
 /* solve_fgmres (src/solver_krylov.cpp:1557-2650) with the MG plan as the
  * (flexible) preconditioner.  recycle: 0 none, 1 capture cycle corrections
  * for the next solve, 2 project the captured ones, 3 initial-guess guard

@@ -25,6 +25,7 @@
 #include <mpi.h>
 
 #include <algorithm>
+#include <memory>
 #include <array>
 #include <chrono>
 #include <cmath>
@@ -33,6 +34,7 @@
 #include <cstring>
 #include <memory>
 #include <vector>
+#include "solver_iccg.hpp"  // ColdPressureIccg, ColdPressureDilu (header classes)
 
 namespace {
 using namespace hundun::v04;
@@ -230,6 +232,11 @@ struct Session {
   LinearAlgorithm algorithm{LinearAlgorithm::pcg};
   std::uint32_t restart{};
   double setup_seconds{};
+  // Cold-path preconditioners on the decorated operator's rows.
+  int preconditioner{};  // 0 MG plan, 1 ColdPressureIccg, 2 ColdPressureDilu
+  std::vector<detail::ColdPressureRow> cold_rows;
+  std::unique_ptr<detail::ColdPressureIccg> iccg;
+  std::unique_ptr<detail::ColdPressureDilu> dilu;
 };
 
 int code_of(Status s) {
@@ -240,10 +247,10 @@ int code_of(Status s) {
 
 extern "C" {
 
-// options: [algorithm(0 pcg,1 fgmres), restart, smoother(0 red-black,
+// options: [algorithm(0 pcg,1 fgmres,2 bicgstab), restart, smoother(0 red-black,
 //           1 chebyshev), cycle(0 V,1 F), pre, post, coarse_sweeps,
 //           scaling(0 residual-minimising, 1 unit_linear), max_levels,
-//           minimum_coarse_extent]
+//           minimum_coarse_extent, preconditioner(0 MG plan, 1 ICCG, 2 DILU)]
 // reals:   [chebyshev_lower_spectrum_fraction, anisotropy_threshold,
 //           diagonal_shortcut_maximum_ratio]
 // Returns 0 on success, otherwise status code * 100000 + detail.
@@ -329,7 +336,10 @@ int hfref_create(int nx, int ny, int nz, const double* x_faces,
         }
   }
 
-  s.algorithm = options[0] == 1 ? LinearAlgorithm::fgmres : LinearAlgorithm::pcg;
+  s.algorithm = options[0] == 1 ? LinearAlgorithm::fgmres
+                 : options[0] == 2 ? LinearAlgorithm::bicgstab
+                                   : LinearAlgorithm::pcg;
+  s.preconditioner = options[10];
   s.restart = s.algorithm == LinearAlgorithm::fgmres
                   ? static_cast<std::uint32_t>(options[1])
                   : 0U;
@@ -427,6 +437,55 @@ int hfref_create(int nx, int ny, int nz, const double* x_faces,
   s.op.fz = s.z_faces.storage.data();
   s.op.active = s.has_activity ? s.active_cells.data() : nullptr;
   s.op.identity = s.identity;
+  if (s.preconditioner != 0) {
+    // Rows of the decorated operator: identity rows on solid cells; a link
+    // to a solid cell or a Neumann boundary face moves its coefficient out
+    // of the row (the neighbour reads the cell itself); Dirichlet boundary
+    // neighbours read zero.  neighbour[2a] / [2a+1] couple to the low /
+    // high neighbour along axis a with the positive face coefficient.
+    s.cold_rows.assign(n, detail::ColdPressureRow{});
+    const Int3 xe{nx + 1, ny, nz}, ye{nx, ny + 1, nz}, ze{nx, ny, nz + 1};
+    const auto on = [&](int i, int j, int k) {
+      return !s.has_activity || s.active_cells[flat(s.cells, i, j, k)] != 0U;
+    };
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+          detail::ColdPressureRow& row = s.cold_rows[flat(s.cells, i, j, k)];
+          if (!on(i, j, k)) {
+            row.diagonal = 1.0;
+            continue;
+          }
+          row.diagonal = s.diagonal[flat(s.cells, i, j, k)];
+          const int c[3]{i, j, k};
+          const int e[3]{nx, ny, nz};
+          const double face[6]{s.op.fx[flat(xe, i, j, k)], s.op.fx[flat(xe, i + 1, j, k)],
+                               s.op.fy[flat(ye, i, j, k)], s.op.fy[flat(ye, i, j + 1, k)],
+                               s.op.fz[flat(ze, i, j, k)], s.op.fz[flat(ze, i, j, k + 1)]};
+          for (int f = 0; f < 6; ++f) {
+            const int a = f / 2;
+            int nb[3]{c[0], c[1], c[2]};
+            nb[a] += (f % 2) ? 1 : -1;
+            if (nb[a] < 0 || nb[a] >= e[a]) {
+              if (boundary_kinds[f] == 1) row.diagonal -= face[f];
+              continue;
+            }
+            if (!on(nb[0], nb[1], nb[2])) {
+              row.diagonal -= face[f];
+              continue;
+            }
+            row.neighbour[f] = face[f];
+          }
+        }
+    if (s.preconditioner == 1) {
+      s.iccg = std::make_unique<detail::ColdPressureIccg>(s.cold_rows, s.cells, s.identity);
+      st = s.iccg->prepare();
+    } else {
+      s.dilu = std::make_unique<detail::ColdPressureDilu>(s.cold_rows, s.cells, s.identity);
+      st = s.dilu->prepare();
+    }
+    if (!st) return code_of(st);
+  }
   s.setup_seconds = std::chrono::duration<double>(
                         std::chrono::steady_clock::now() - begin)
                         .count();
@@ -484,7 +543,29 @@ int hfref_apply_mg(void* handle, const double* r, double* z) {
   return st ? 0 : code_of(st);
 }
 
-// Runs solve_pcg (adapter-certified MG) or solve_fgmres (MG as given).
+// One application of the cold-path preconditioner (ICCG or DILU).
+int hfref_apply_cold(void* handle, const double* r, double* z) {
+  Session& s = *static_cast<Session*>(handle);
+  if (s.preconditioner == 0) return 1;
+  OwnedField in = make_field(46U, s.cells, 0U, 1U, 306U, 406U);
+  OwnedField out = make_field(47U, s.cells, 0U, 1U, 307U, 407U);
+  for (int k = 0; k < s.cells.z; ++k)
+    for (int j = 0; j < s.cells.y; ++j)
+      for (int i = 0; i < s.cells.x; ++i)
+        in.view.unchecked({i, j, k}, 0U) = r[flat(s.cells, i, j, k)];
+  LinearPreconditioner* pc = s.preconditioner == 1
+                                 ? static_cast<LinearPreconditioner*>(s.iccg.get())
+                                 : static_cast<LinearPreconditioner*>(s.dilu.get());
+  const Status st = pc->apply(as_const(in.view), out.view, 0U);
+  for (int k = 0; k < s.cells.z; ++k)
+    for (int j = 0; j < s.cells.y; ++j)
+      for (int i = 0; i < s.cells.x; ++i)
+        z[flat(s.cells, i, j, k)] = out.view.unchecked({i, j, k}, 0U);
+  return st ? 0 : code_of(st);
+}
+
+// Runs solve_pcg (adapter-certified MG, or ICCG), solve_bicgstab (DILU) or
+// solve_fgmres (MG as given).
 // recycle (FGMRES): 0 none (clears any recycle session), 1 begin a capture
 // session (corrector 1: SolverWorkspace::recycle_begin_capture), 2 project
 // the captured corrections (corrector 2: recycle_begin_projection), 3 the
@@ -537,10 +618,17 @@ int hfref_solve(void* handle, const double* rhs, double* solution,
       static_cast<std::uint32_t>(true_residual_interval);
   invocation.control.restart = s.restart;
   const auto begin = std::chrono::steady_clock::now();
+  LinearPreconditioner* pc =
+      s.preconditioner == 1 ? static_cast<LinearPreconditioner*>(s.iccg.get())
+      : s.preconditioner == 2 ? static_cast<LinearPreconditioner*>(s.dilu.get())
+      : s.algorithm == LinearAlgorithm::pcg ? static_cast<LinearPreconditioner*>(&s.adapter)
+                                            : static_cast<LinearPreconditioner*>(&s.plan);
   const LinearSolveResult result =
       s.algorithm == LinearAlgorithm::pcg
-          ? solve_pcg(s.op, s.adapter, invocation, s.workspace, s.reductions)
-          : solve_fgmres(s.op, s.plan, invocation, s.workspace, s.reductions);
+          ? solve_pcg(s.op, *pc, invocation, s.workspace, s.reductions)
+      : s.algorithm == LinearAlgorithm::bicgstab
+          ? solve_bicgstab(s.op, *pc, invocation, s.workspace, s.reductions)
+          : solve_fgmres(s.op, *pc, invocation, s.workspace, s.reductions);
   const double seconds =
       std::chrono::duration<double>(std::chrono::steady_clock::now() - begin)
           .count();

@@ -38,6 +38,7 @@ def _load():
         lib.hfref_levels.restype = ctypes.c_int
         lib.hfref_apply_operator.argtypes = [ctypes.c_void_p, dp, dp]
         lib.hfref_apply_mg.argtypes = [ctypes.c_void_p, dp, dp]
+        lib.hfref_apply_cold.argtypes = [ctypes.c_void_p, dp, dp]
         lib.hfref_solve.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int, dp]
         _lib = lib
@@ -81,8 +82,15 @@ class RefSession:
                    "operator_failure", "preconditioner_failure", "collective_failure",
                    "invalid_plan", "convergence_audit_failure"]
 
+    PRECONDITIONERS = {"mg": 0, "iccg": 1, "dilu": 2}
+    ALGORITHMS = {"pcg": 0, "fgmres": 1, "bicgstab": 2}
+
     def __init__(self, system, policy: Optional[MgPolicy] = None, algorithm: str = "pcg",
-                 restart: int = 12, unit_linear: Optional[bool] = None):
+                 restart: int = 12, unit_linear: Optional[bool] = None,
+                 preconditioner: str = "mg"):
+        """``algorithm`` "pcg" / "fgmres" / "bicgstab"; ``preconditioner`` "mg"
+        (the plan), "iccg" (ColdPressureIccg, with PCG) or "dilu"
+        (ColdPressureDilu, with BiCGSTAB)."""
         lib = _load()
         self.system = system
         policy = policy or MgPolicy()
@@ -91,10 +99,11 @@ class RefSession:
         nx, ny, nz = system.shape
         self._faces = [np.ascontiguousarray(f, dtype=np.float64) for f in system.faces]
         self._bc = (ctypes.c_int * 6)(*system.boundary)
-        options = (ctypes.c_int * 10)(1 if algorithm == "fgmres" else 0, restart, policy.smoother,
+        options = (ctypes.c_int * 11)(self.ALGORITHMS[algorithm], restart, policy.smoother,
                                       policy.cycle, policy.pre, policy.post, policy.coarse_sweeps,
                                       1 if unit_linear else 0, policy.max_levels,
-                                      policy.min_coarse_extent)
+                                      policy.min_coarse_extent,
+                                      self.PRECONDITIONERS[preconditioner])
         reals = (ctypes.c_double * 3)(policy.chebyshev_fraction, policy.anisotropy_threshold,
                                       policy.diagonal_shortcut)
         active = None
@@ -130,6 +139,15 @@ class RefSession:
         if rc != 0:
             raise RuntimeError(f"reference operator failed: {rc}")
         return y
+
+    def apply_cold(self, r: np.ndarray) -> np.ndarray:
+        """One application of the cold-path preconditioner (ICCG or DILU)."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.empty_like(r)
+        rc = self._lib.hfref_apply_cold(self._handle, _dp(r), _dp(z))
+        if rc != 0:
+            raise RuntimeError(f"reference cold preconditioner failed: {rc}")
+        return z
 
     def apply_mg(self, r: np.ndarray) -> np.ndarray:
         r = np.ascontiguousarray(r, dtype=np.float64)

@@ -121,6 +121,28 @@ def main():
         }
     np.savez_compressed(os.path.join(HERE, "recycle_sphere_24x20x16_prodF.npz"), **arrays)
     index[name]["recycle"] = recycle
+
+    # Cold path: solve_pcg with ColdPressureIccg and solve_bicgstab with
+    # ColdPressureDilu on the decorated operator (src/solver_iccg.hpp:224-293,
+    # src/solver_cold.hpp:484-560; src/solver_krylov.cpp:2651-3090).
+    cold_arrays = {}
+    for name in ("sphere_24x20x16_rbV22", "wrinkled_16x40x12_lineF"):
+        spec, pol = CASES[name]
+        system = system_for(spec)
+        v = probe_vector(system)
+        entry = {}
+        for algorithm, pc in (("pcg", "iccg"), ("bicgstab", "dilu")):
+            ref = ref_oracle.RefSession(system, ref_oracle.MgPolicy(**pol), algorithm=algorithm,
+                                        preconditioner=pc)
+            cold_arrays[f"{name}_{pc}_apply"] = ref.apply_cold(v)
+            x, info = ref.solve(system.rhs, rtol=1e-10, maxit=4000)
+            ref.close()
+            cold_arrays[f"{name}_{algorithm}_{pc}_x"] = x
+            entry[f"{algorithm}_{pc}"] = {"iterations": info["iterations"],
+                                         "termination": info["termination"],
+                                         "operator_applies": info["operator_applies"]}
+        index[name]["cold"] = entry
+    np.savez_compressed(os.path.join(HERE, "cold_path.npz"), **cold_arrays)
     with open(os.path.join(HERE, "index.json"), "w") as f:
         json.dump(index, f, indent=1)
 

@@ -263,3 +263,41 @@ def test_zero_rhs_and_converged_guess():
     x1, _ = o.solve(s.rhs, rtol=1e-12)
     x2, info2 = o.solve(s.rhs, x0=x1, rtol=1e-10)
     assert info2["iterations"] == 0 and info2["termination"] == "converged"
+
+
+@pytest.mark.parametrize("name", ["sphere_24x20x16_rbV22", "wrinkled_16x40x12_lineF"])
+def test_cold_path_restatement_reproduces_reference_golden(name):
+    """Diagonal IC(0) in lexicographic order (ColdPressureIccg,
+    src/solver_iccg.hpp:224-293; ColdPressureDilu, src/solver_cold.hpp:
+    484-560, identical on the symmetric pressure rows) with solve_pcg and
+    solve_bicgstab (src/solver_krylov.cpp:2651-3090), bit for bit."""
+    import c_oracle
+    s = golden_cases.system(name)
+    meta = golden_cases.index()[name]["cold"]
+    gold = np.load(os.path.join(golden_cases.GOLDEN, "cold_path.npz"))
+    o = c_oracle.OracleSession(s, golden_cases.policy(name), preconditioner="dic")
+    v = golden_cases.probe(s)
+    z = o.apply_preconditioner(v)
+    assert np.array_equal(z, gold[f"{name}_iccg_apply"])
+    assert np.array_equal(z, gold[f"{name}_dilu_apply"])
+    for algorithm, pc in (("pcg", "iccg"), ("bicgstab", "dilu")):
+        x, info = o.solve(s.rhs, rtol=1e-10, maxit=4000, algorithm=algorithm)
+        assert info["iterations"] == meta[f"{algorithm}_{pc}"]["iterations"]
+        assert info["operator_applies"] == meta[f"{algorithm}_{pc}"]["operator_applies"]
+        assert np.array_equal(x, gold[f"{name}_{algorithm}_{pc}_x"])
+
+
+def test_cold_path_matches_live_reference_with_ibm():
+    import c_oracle
+    import ref_oracle
+    if not ref_oracle.available():
+        pytest.skip("compiled reference not built (make -C oracle ref)")
+    s = workloads.make("sphere64", n=(15, 12, 10), seed=12)
+    pol = ref_oracle.MgPolicy()
+    o = c_oracle.OracleSession(s, pol, preconditioner="dic")
+    for algorithm, pc in (("pcg", "iccg"), ("bicgstab", "dilu")):
+        r = ref_oracle.RefSession(s, pol, algorithm=algorithm, preconditioner=pc)
+        x1, i1 = r.solve(s.rhs, rtol=1e-9, maxit=3000)
+        x2, i2 = o.solve(s.rhs, rtol=1e-9, maxit=3000, algorithm=algorithm)
+        assert i1["iterations"] == i2["iterations"]
+        assert np.array_equal(x1, x2)
