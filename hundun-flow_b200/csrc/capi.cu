@@ -51,6 +51,7 @@ void hfps_default_policy(hfps_policy* p) {
   p->chebyshev_lower_spectrum_fraction = 0.3;
   p->anisotropy_threshold = 4.0;
   p->diagonal_shortcut_maximum_ratio = 0.0;
+  p->preconditioner = HFPS_PRECONDITIONER_MG;
 }
 
 void hfps_production_policy(hfps_policy* p) {

@@ -551,6 +551,165 @@ __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
 }
 
 // ---------------------------------------------------------------------------
+// Cold-path diagonal IC(0) (ColdPressureIccg, src/solver_iccg.hpp:224-293;
+// ColdPressureDilu, src/solver_cold.hpp:484-560, identical on the symmetric
+// pressure rows).  The factorisation and both triangular sweeps follow the
+// reference's lexicographic order exactly: a cell depends only on its lower
+// (resp. upper) neighbours, which all lie on the previous wavefront plane
+// i + j + k = t - 1 (resp. t + 1), so every plane is one parallel launch and
+// each cell's arithmetic is the reference's, operation for operation.  The
+// couplings are the IBM-masked level-0 face coefficients.
+
+// Row diagonal of the decorated operator: identity on solid cells; a link to
+// a solid cell or a Neumann boundary face leaves the row and its coefficient
+// is subtracted from the diagonal, in face order x-, x+, y-, y+, z-, z+.
+__global__ void k_dic_rows(int nx, int ny, int nz, unsigned neumann, const double* diag,
+                           const double* fx, const double* fy, const double* fz,
+                           const uint8_t* active, double* out) {
+  grid_dependency_sync();
+  const int n = nx * ny * nz;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    int i, j, k;
+    cell_coords(c, nx, ny, i, j, k);
+    const auto on = [&](int q) { return active == nullptr || active[q] != 0; };
+    if (!on(c)) {
+      out[c] = 1.0;
+      continue;
+    }
+    const int fxi = c + j + ny * k;
+    const int fyi = c + nx * k;
+    const int plane = nx * ny;
+    const double face[6] = {fx[fxi], fx[fxi + 1], fy[fyi], fy[fyi + nx], fz[c], fz[c + plane]};
+    const int at[3] = {i, j, k};
+    const int ext[3] = {nx, ny, nz};
+    const int step[3] = {1, nx, plane};
+    double d = diag[c];
+    for (int f = 0; f < 6; ++f) {
+      const int a = f >> 1;
+      const int q = at[a] + ((f & 1) ? 1 : -1);
+      if (q < 0 || q >= ext[a]) {
+        if ((neumann >> f) & 1u) d -= face[f];
+        continue;
+      }
+      if (!on((f & 1) ? c + step[a] : c - step[a])) d -= face[f];
+    }
+    out[c] = d;
+  }
+}
+
+// Cell (i, j, k) of wavefront plane t handled by this thread, or false.
+__device__ __forceinline__ bool plane_cell(int t, int nx, int ny, int nz, int& i, int& j,
+                                           int& k) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ny * nz) return false;
+  k = q / ny;
+  j = q - k * ny;
+  i = t - j - k;
+  return i >= 0 && i < nx;
+}
+
+__global__ void k_dic_pivots(int t, Level<double> L, const double* rows, double* inv,
+                             Scalars* scalars) {
+  grid_dependency_sync();
+  int i, j, k;
+  if (!plane_cell(t, L.nx, L.ny, L.nz, i, j, k)) return;
+  const int c = i + L.nx * (j + L.ny * k);
+  const int plane = L.nx * L.ny;
+  double pivot = rows[c];
+  // lower couplings: the cell's own x-, y-, z- faces
+  if (i > 0) {
+    const double lower = L.fx[face_x_index(L, c, j, k)];
+    pivot -= lower * lower * inv[c - 1];
+  }
+  if (j > 0) {
+    const double lower = L.fy[face_y_index(L, c, k)];
+    pivot -= lower * lower * inv[c - L.nx];
+  }
+  if (k > 0) {
+    const double lower = L.fz[c];
+    pivot -= lower * lower * inv[c - plane];
+  }
+  if (!(pivot > 0) || !isfinite(pivot)) atomicOr(&scalars->flags, 1);
+  inv[c] = 1 / pivot;
+}
+
+__global__ void k_dic_forward(int t, Level<double> L, const double* in, double* out,
+                              const double* inv) {
+  grid_dependency_sync();
+  int i, j, k;
+  if (!plane_cell(t, L.nx, L.ny, L.nz, i, j, k)) return;
+  const int c = i + L.nx * (j + L.ny * k);
+  double value = in[c];
+  if (i > 0) value += L.fx[face_x_index(L, c, j, k)] * out[c - 1];
+  if (j > 0) value += L.fy[face_y_index(L, c, k)] * out[c - L.nx];
+  if (k > 0) value += L.fz[c] * out[c - L.nx * L.ny];
+  out[c] = value * inv[c];
+}
+
+__global__ void k_dic_backward(int t, Level<double> L, double* out, const double* inv) {
+  grid_dependency_sync();
+  int i, j, k;
+  if (!plane_cell(t, L.nx, L.ny, L.nz, i, j, k)) return;
+  const int c = i + L.nx * (j + L.ny * k);
+  const int plane = L.nx * L.ny;
+  double value = 0;
+  // upper couplings: the lower face of the next cell along each axis
+  if (i + 1 < L.nx) value += L.fx[face_x_index(L, c, j, k) + 1] * out[c + 1];
+  if (j + 1 < L.ny) value += L.fy[face_y_index(L, c, k) + L.nx] * out[c + L.nx];
+  if (k + 1 < L.nz) value += L.fz[c + plane] * out[c + plane];
+  out[c] += value * inv[c];
+}
+
+// ---------------------------------------------------------------------------
+// BiCGSTAB kernels (solve_bicgstab, src/solver_krylov.cpp:2651-3090), in the
+// reference's per-cell arithmetic.
+
+// p = 1.0 r + beta (1.0 p - omega v) (update_bicgstab_search_direction).
+__global__ void k_bicg_direction(int n, double* __restrict__ p, const double* __restrict__ r,
+                                 const double* __restrict__ v, double beta, double omega) {
+  grid_dependency_sync();
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const double intermediate = 1.0 * p[c] + -omega * v[c];
+    p[c] = 1.0 * r[c] + beta * intermediate;
+  }
+}
+
+// s = 1.0 r - alpha v and |s|^2 (form_bicgstab_intermediate).
+__global__ void k_bicg_intermediate(int n, double* __restrict__ s, const double* __restrict__ r,
+                                    const double* __restrict__ v, double alpha, Reduce red) {
+  grid_dependency_sync();
+  double acc[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const double value = 1.0 * r[c] + -alpha * v[c];
+    s[c] = value;
+    acc[0] += value * value;
+  }
+  if (finish_reduction<1>(acc, red) && threadIdx.x == 0) apply_scalar_op(red.scalars, red.op, acc[0]);
+}
+
+// x = (x + alpha ph) + omega sh, r = 1.0 s - omega t and |r|^2
+// (update_bicgstab_solution_residual).
+__global__ void k_bicg_update(int n, double* __restrict__ x, const double* __restrict__ ph,
+                              const double* __restrict__ sh, double* __restrict__ r,
+                              const double* __restrict__ s, const double* __restrict__ t,
+                              double alpha, double omega, Reduce red) {
+  grid_dependency_sync();
+  double acc[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const double intermediate = x[c] + alpha * ph[c];
+    x[c] = intermediate + omega * sh[c];
+    const double value = 1.0 * s[c] + -omega * t[c];
+    r[c] = value;
+    acc[0] += value * value;
+  }
+  if (finish_reduction<1>(acc, red) && threadIdx.x == 0) apply_scalar_op(red.scalars, red.op, acc[0]);
+}
+
+// ---------------------------------------------------------------------------
 // FGMRES kernels (solve_fgmres, src/solver_krylov.cpp:1557-2650).
 
 // w = A z + (-shift) v: the operator image of the preconditioned basis
@@ -1249,6 +1408,42 @@ void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red) {
 void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc) {
   launch(k_p_update, grid_for(n), kThreads, 0, s, n, p, z, sc);
+}
+void launch_dic_rows(cudaStream_t s, int nx, int ny, int nz, unsigned neumann,
+                     const double* diag, const double* fx, const double* fy, const double* fz,
+                     const uint8_t* active, double* out) {
+  launch(k_dic_rows, grid_for(static_cast<long long>(nx) * ny * nz), kThreads, 0, s, nx, ny, nz,
+         neumann, diag, fx, fy, fz, active, out);
+}
+int dic_planes(const Level<double>& L) { return L.nx + L.ny + L.nz - 2; }
+static int plane_blocks(const Level<double>& L) {
+  return static_cast<int>((static_cast<long long>(L.ny) * L.nz + kThreads - 1) / kThreads);
+}
+void launch_dic_pivots(cudaStream_t s, const Level<double>& L, const double* rows, double* inv,
+                       Scalars* scalars) {
+  for (int t = 0; t < dic_planes(L); ++t)
+    launch(k_dic_pivots, plane_blocks(L), kThreads, 0, s, t, L, rows, inv, scalars);
+}
+void launch_dic_apply(cudaStream_t s, const Level<double>& L, const double* in, double* out,
+                      const double* inv) {
+  for (int t = 0; t < dic_planes(L); ++t)
+    launch(k_dic_forward, plane_blocks(L), kThreads, 0, s, t, L, in, out, inv);
+  for (int t = dic_planes(L) - 1; t >= 0; --t)
+    launch(k_dic_backward, plane_blocks(L), kThreads, 0, s, t, L, out, inv);
+}
+void launch_bicg_direction(cudaStream_t s, int n, double* p, const double* r, const double* v,
+                           double beta, double omega) {
+  launch(k_bicg_direction, grid_for(n), kThreads, 0, s, n, p, r, v, beta, omega);
+}
+void launch_bicg_intermediate(cudaStream_t s, int n, double* sv, const double* r,
+                              const double* v, double alpha, Reduce red) {
+  launch(k_bicg_intermediate, reduction_blocks(n), kThreads, 0, s, n, sv, r, v, alpha, red);
+}
+void launch_bicg_update(cudaStream_t s, int n, double* x, const double* ph, const double* sh,
+                        double* r, const double* sv, const double* t, double alpha,
+                        double omega, Reduce red) {
+  launch(k_bicg_update, reduction_blocks(n), kThreads, 0, s, n, x, ph, sh, r, sv, t, alpha,
+         omega, red);
 }
 void launch_operator_shift(cudaStream_t s, const Level<double>& L, const double* z,
                            const double* v, double shift, double* w) {

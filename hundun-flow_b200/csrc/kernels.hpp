@@ -162,6 +162,28 @@ void launch_correct_flux(cudaStream_t s, int nx, int ny, int nz, unsigned neuman
                          const double* p, const double* cx, const double* cy,
                          const double* cz, double scale, double* qx, double* qy, double* qz,
                          Scalars* scalars);
+// ---- cold path: diagonal IC(0) and BiCGSTAB ----------------------------------
+// Decorated-row diagonal of the cold-path factorisation.
+void launch_dic_rows(cudaStream_t s, int nx, int ny, int nz, unsigned neumann,
+                     const double* diag, const double* fx, const double* fy, const double* fz,
+                     const uint8_t* active, double* out);
+// Wavefront planes i + j + k = t of a level: nx + ny + nz - 2.
+int dic_planes(const Level<double>& L);
+// Inverse pivots, plane by plane (flags bit 0 on a non-positive pivot).
+void launch_dic_pivots(cudaStream_t s, const Level<double>& L, const double* rows, double* inv,
+                       Scalars* scalars);
+// out = M^{-1} in: forward then backward sweep, plane by plane.
+void launch_dic_apply(cudaStream_t s, const Level<double>& L, const double* in, double* out,
+                      const double* inv);
+void launch_bicg_direction(cudaStream_t s, int n, double* p, const double* r, const double* v,
+                           double beta, double omega);
+// s = r - alpha v, with |s|^2 through red.
+void launch_bicg_intermediate(cudaStream_t s, int n, double* sv, const double* r,
+                              const double* v, double alpha, Reduce red);
+// x = (x + alpha ph) + omega sh, r = s - omega t, with |r|^2 through red.
+void launch_bicg_update(cudaStream_t s, int n, double* x, const double* ph, const double* sh,
+                        double* r, const double* sv, const double* t, double alpha,
+                        double omega, Reduce red);
 // ---- FGMRES (solve_fgmres) ---------------------------------------------------
 // Basis vectors handled by one multidot / basis-update launch.
 constexpr int kBasisChunk = 16;

@@ -95,6 +95,8 @@ bool valid_policy(const hfps_policy& p) {
          std::isfinite(p.chebyshev_lower_spectrum_fraction) &&
          p.chebyshev_lower_spectrum_fraction > 0.0 &&
          p.chebyshev_lower_spectrum_fraction < 1.0 &&
+         (p.preconditioner == HFPS_PRECONDITIONER_MG ||
+          p.preconditioner == HFPS_PRECONDITIONER_IC0) &&
          std::isfinite(p.diagonal_shortcut_maximum_ratio) &&
          p.diagonal_shortcut_maximum_ratio >= 0.0 &&
          p.diagonal_shortcut_maximum_ratio < 1.0 &&
@@ -120,6 +122,7 @@ Solver::~Solver() {
   if (stream_ != nullptr) cudaStreamSynchronize(stream_);
   for (auto& g : mg_graph_)
     if (g != nullptr) cudaGraphExecDestroy(g);
+  if (dic_graph_ != nullptr) cudaGraphExecDestroy(dic_graph_);
   if (h_scalars_ != nullptr) cudaFreeHost(h_scalars_);
   if (arena_ != nullptr) cudaFree(arena_);
   if (fg_storage_ != nullptr) cudaFree(fg_storage_);
@@ -279,6 +282,11 @@ Status Solver::allocate() {
       dense_off = add(2 * static_cast<size_t>(last_cells) * last_cells * 8);
     }
   }
+  size_t dic_off[2] = {SIZE_MAX, SIZE_MAX};
+  if (policy_.preconditioner == HFPS_PRECONDITIONER_IC0) {
+    dic_off[0] = add(cells * 8);
+    dic_off[1] = add(cells * 8);
+  }
   arena_bytes_ = bytes;
   Status st = check(cudaMalloc(&arena_, arena_bytes_), "device arena");
   if (!st) return st;
@@ -314,6 +322,10 @@ Status Solver::allocate() {
   d_scalars_ = reinterpret_cast<Scalars*>(at(scalars_off));
   d_partials_ = reinterpret_cast<double*>(at(partials_off));
   coarse_op_ = dense_off == SIZE_MAX ? nullptr : reinterpret_cast<double*>(at(dense_off));
+  if (dic_off[0] != SIZE_MAX) {
+    dic_rows_ = reinterpret_cast<double*>(at(dic_off[0]));
+    dic_inv_ = reinterpret_cast<double*>(at(dic_off[1]));
+  }
   l64_.resize(levels);
   l32_.resize(levels);
   volume_.resize(levels);
@@ -481,7 +493,30 @@ Status Solver::build_hierarchy() {
     if (gexec != nullptr) cudaGraphExecDestroy(gexec);
     gexec = nullptr;
   }
-  return check(cudaStreamSynchronize(stream_), "hierarchy");
+  st = check(cudaStreamSynchronize(stream_), "hierarchy");
+  if (!st) return st;
+  return dic_factor();
+}
+
+// Cold-path IC(0) factorisation from the coefficients still staged in
+// user_ (diagonal, unmasked faces): decorated row diagonals, then the
+// inverse pivots plane by plane (ColdPressureIccg::prepare,
+// src/solver_iccg.hpp:236-256).
+Status Solver::dic_factor() {
+  if (dic_rows_ == nullptr) return {};
+  const Level<double> L0 = l64_[0].view(neumann_);
+  Status st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  launch_dic_rows(stream_, nx_, ny_, nz_, neumann_, user_[0], user_[1], user_[2], user_[3],
+                  d_active_, dic_rows_);
+  launch_dic_pivots(stream_, L0, dic_rows_, dic_inv_, d_scalars_);
+  st = sync_scalars();
+  if (!st) return st;
+  if (h_scalars_->flags & 1) {
+    coefficients_ready_ = false;
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "IC(0) pivot not positive");
+  }
+  return {};
 }
 
 Status Solver::refresh_mixed() {
@@ -795,6 +830,35 @@ Status Solver::mg_apply(bool mixed) {
   return check(cudaGraphLaunch(mg_graph_[slot], stream_), "graph launch");
 }
 
+Status Solver::dic_apply() {
+  const Level<double> L0 = l64_[0].view(neumann_);
+  if (!use_graphs_) {
+    launch_dic_apply(stream_, L0, kr_, kz_, dic_inv_);
+    launches_ += 2 * static_cast<uint64_t>(dic_planes(L0));
+    return check(cudaGetLastError(), "IC(0) launch");
+  }
+  if (dic_graph_ == nullptr) {
+    cudaGraph_t graph = nullptr;
+    Status st = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal),
+                      "graph capture begin");
+    if (!st) return st;
+    launch_dic_apply(stream_, L0, kr_, kz_, dic_inv_);
+    st = check(cudaStreamEndCapture(stream_, &graph), "graph capture end");
+    if (!st) return st;
+    cudaGraphGetNodes(graph, nullptr, &dic_nodes_);
+    st = check(cudaGraphInstantiate(&dic_graph_, graph, 0), "graph instantiate");
+    cudaGraphDestroy(graph);
+    if (!st) return st;
+  }
+  launches_ += dic_nodes_;
+  return check(cudaGraphLaunch(dic_graph_, stream_), "graph launch");
+}
+
+Status Solver::precondition(bool mixed) {
+  if (policy_.preconditioner == HFPS_PRECONDITIONER_IC0) return dic_apply();
+  return mg_apply(mixed);
+}
+
 Status Solver::sync_scalars() {
   Status st = check(cudaMemcpyAsync(h_scalars_, d_scalars_, sizeof(Scalars),
                                     cudaMemcpyDeviceToHost, stream_),
@@ -850,7 +914,7 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
     return {};
   }
   const auto restart_direction = [&]() -> Status {
-    Status s = mg_apply(mixed);
+    Status s = precondition(mixed);
     if (!s) return s;
     ++result.preconditioner_applies;
     launch_dot(stream_, n, kr_, kz_, red(kOpRhoRestart));
@@ -909,7 +973,7 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
       if (!st) return st;
       continue;
     }
-    st = mg_apply(mixed);
+    st = precondition(mixed);
     if (!st) return st;
     ++result.preconditioner_applies;
     launch_dot(stream_, n, kr_, kz_, red(kOpRhoNext));
@@ -1292,7 +1356,7 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
       // z_j = M v_j through the MG graph's fixed input/output buffers.
       launch_copy(stream_, n, V[column], kr_);
       launches_ += 1;
-      st = mg_apply(mixed);
+      st = precondition(mixed);
       if (!st) return st;
       ++result.preconditioner_applies;
       launch_copy(stream_, n, kz_, Z[column]);
@@ -1445,6 +1509,209 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
   return fail(HFPS_REJECTED_STEP, kDetailBreakdown, "maximum iterations reached");
 }
 
+// solve_bicgstab (src/solver_krylov.cpp:2651-3090) with the default
+// control (no bounded recurrence, no maximum norm, no best-iterate
+// retention): the early exit when |s| meets the tolerance, omega from the
+// (t.s, t.t) pair, a true residual every true_residual_interval iterations
+// and at a recursive claim, and a fresh start (r_hat = r) after every
+// verification that does not converge.  The preconditioner runs on the
+// kr_ -> kz_ buffers; the BiCGSTAB vectors live in the FGMRES basis block.
+Status Solver::krylov_bicgstab(const hfps_control& control, hfps_result& result,
+                               double* history, uint32_t capacity) {
+  const int n = nx_ * ny_ * nz_;
+  const Level<double> A = l64_[0].view(neumann_);
+  const auto red = [&](int op) { return Reduce{d_scalars_, d_partials_, op}; };
+  Status st = ensure_fgmres_storage(4);
+  if (!st) return st;
+  double* rh = fg_v_[0];
+  double* p = fg_v_[1];
+  double* sv = fg_v_[2];
+  double* ph = fg_v_[3];
+  double* sh = fg_v_[4];
+  double* v = fg_z_[0];
+  double* t = fg_z_[1];
+  double* r = fg_z_[2];
+  st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
+  if (!st) return st;
+  launch_norm2(stream_, n, kb_, red(kOpMisc));
+  launches_ += 1;
+  st = sync_scalars();
+  if (!st) return st;
+  if (h_scalars_->flags & 1) {
+    result.termination = HFPS_NON_FINITE;
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite rhs");
+  }
+  const double bnorm = std::sqrt(h_scalars_->misc[0]);
+  const double tol = std::max(control.absolute_tolerance, control.relative_tolerance * bnorm);
+  result.rhs_norm = bnorm;
+  result.true_residual_limit = tol;
+  if (bnorm == 0.0) {
+    st = check(cudaMemsetAsync(kx_, 0, n * sizeof(double), stream_), "zero x");
+    result.termination = HFPS_ZERO_RHS;
+    return st;
+  }
+  const auto true_residual = [&](double& norm) -> Status {
+    launch_residual_norm(stream_, A, kx_, kb_, r, red(kOpRecursive));
+    launches_ += 1;
+    ++result.operator_applies;
+    Status s2 = sync_scalars();
+    if (!s2) return s2;
+    norm = std::sqrt(h_scalars_->rr);
+    if (!std::isfinite(norm)) {
+      result.termination = HFPS_NON_FINITE;
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite residual");
+    }
+    return {};
+  };
+  const auto dots = [&](std::initializer_list<const double*> left, const double* w) -> Status {
+    BasisRefs refs{};
+    refs.count = 0;
+    for (const double* l : left) refs.v[refs.count++] = l;
+    launch_multidot(stream_, n, refs, w, false, d_scalars_->hcol, red(kCounterMultidot));
+    launches_ += 1;
+    return sync_scalars();
+  };
+  const auto precondition_into = [&](const double* in, double* out) -> Status {
+    launch_copy(stream_, n, in, kr_);
+    launches_ += 1;
+    Status s2 = precondition(false);
+    if (!s2) return s2;
+    ++result.preconditioner_applies;
+    launch_copy(stream_, n, kz_, out);
+    launches_ += 1;
+    return {};
+  };
+  const auto breakdown = [&]() {
+    result.termination = HFPS_BREAKDOWN;
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailBreakdown, "BiCGSTAB breakdown");
+  };
+  double initial = 0.0;
+  st = true_residual(initial);
+  if (!st) return st;
+  result.initial_true_residual = initial;
+  result.final_true_residual = initial;
+  result.recursive_residual = initial;
+  if (initial <= tol) {
+    result.termination = HFPS_CONVERGED;
+    return {};
+  }
+  launch_copy(stream_, n, r, rh);
+  launches_ += 1;
+  double rho_prev = 1.0, alpha = 1.0, omega = 1.0;
+  bool fresh = true;
+  uint32_t it = 0;
+  const auto record = [&](double value) {
+    result.recursive_residual = value;
+    if (history != nullptr && it - 1 < capacity) {
+      history[it - 1] = value;
+      result.history_length = it;
+    }
+  };
+  while (it < control.maximum_iterations) {
+    st = dots({rh}, r);
+    if (!st) return st;
+    const double rho = h_scalars_->hcol[0];
+    if (rho == 0.0 || !std::isfinite(rho)) return breakdown();
+    if (fresh) {
+      launch_copy(stream_, n, r, p);
+      launches_ += 1;
+    } else {
+      if (omega == 0.0 || !std::isfinite(omega)) return breakdown();
+      const double beta = (rho / rho_prev) * (alpha / omega);
+      launch_bicg_direction(stream_, n, p, r, v, beta, omega);
+      launches_ += 1;
+    }
+    st = precondition_into(p, ph);
+    if (!st) return st;
+    launch_level_apply<double>(stream_, A, ph, v);
+    launches_ += 1;
+    ++result.operator_applies;
+    st = dots({rh}, v);
+    if (!st) return st;
+    const double denominator = h_scalars_->hcol[0];
+    if (denominator == 0.0 || !std::isfinite(denominator)) return breakdown();
+    alpha = rho / denominator;
+    launch_bicg_intermediate(stream_, n, sv, r, v, alpha, red(kOpMisc));
+    launches_ += 1;
+    st = sync_scalars();
+    if (!st) return st;
+    const double s_norm = std::sqrt(h_scalars_->misc[0]);
+    if (!std::isfinite(s_norm)) {
+      result.termination = HFPS_NON_FINITE;
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite BiCGSTAB residual");
+    }
+    if (s_norm <= tol) {
+      BasisRefs one{};
+      one.count = 1;
+      one.v[0] = ph;
+      one.s[0] = alpha;
+      launch_basis_update(stream_, n, kx_, one, 1.0, false, kx_);
+      launches_ += 1;
+      ++it;
+      result.iterations = it;
+      double norm = 0.0;
+      st = true_residual(norm);
+      if (!st) return st;
+      result.final_true_residual = norm;
+      record(norm);
+      if (norm <= tol) {
+        result.termination = HFPS_CONVERGED;
+        return {};
+      }
+      if (it == control.maximum_iterations) break;
+      launch_copy(stream_, n, r, rh);
+      launches_ += 1;
+      rho_prev = 1.0; alpha = 1.0; omega = 1.0; fresh = true;
+      continue;
+    }
+    st = precondition_into(sv, sh);
+    if (!st) return st;
+    launch_level_apply<double>(stream_, A, sh, t);
+    launches_ += 1;
+    ++result.operator_applies;
+    st = dots({sv, t}, t);
+    if (!st) return st;
+    const double ts = h_scalars_->hcol[0], tt = h_scalars_->hcol[1];
+    if (!(tt > 0.0) || !std::isfinite(ts) || !std::isfinite(tt)) return breakdown();
+    omega = ts / tt;
+    if (omega == 0.0 || !std::isfinite(omega)) return breakdown();
+    launch_bicg_update(stream_, n, kx_, ph, sh, r, sv, t, alpha, omega, red(kOpRecursive));
+    launches_ += 1;
+    ++it;
+    result.iterations = it;
+    st = sync_scalars();
+    if (!st) return st;
+    const double recursive = std::sqrt(h_scalars_->rr);
+    if (!std::isfinite(recursive)) {
+      result.termination = HFPS_NON_FINITE;
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite BiCGSTAB residual");
+    }
+    record(recursive);
+    const bool verify = recursive <= tol || it % control.true_residual_interval == 0 ||
+                        it == control.maximum_iterations;
+    if (verify) {
+      double norm = 0.0;
+      st = true_residual(norm);
+      if (!st) return st;
+      result.final_true_residual = norm;
+      result.recursive_residual = norm;
+      if (norm <= tol) {
+        result.termination = HFPS_CONVERGED;
+        return {};
+      }
+      if (it == control.maximum_iterations) break;
+      launch_copy(stream_, n, r, rh);
+      launches_ += 1;
+      rho_prev = 1.0; alpha = 1.0; omega = 1.0; fresh = true;
+      continue;
+    }
+    rho_prev = rho;
+    fresh = false;
+  }
+  result.termination = HFPS_MAXIMUM_ITERATIONS;
+  return fail(HFPS_REJECTED_STEP, kDetailBreakdown, "maximum iterations reached");
+}
+
 Status Solver::solve(const double* rhs, double* solution, int memory,
                      const hfps_control& control, hfps_result& result,
                      double* history, uint32_t capacity) {
@@ -1463,7 +1730,11 @@ Status Solver::solve(const double* rhs, double* solution, int memory,
       (control.precision != HFPS_FP64 && control.precision != HFPS_MIXED) ||
       control.recycle < HFPS_RECYCLE_NONE || control.recycle > HFPS_RECYCLE_GUARD ||
       (control.algorithm == HFPS_PCG && control.recycle != HFPS_RECYCLE_NONE) ||
-      !((control.algorithm == HFPS_PCG && control.restart == 0 && policy_.unit_linear) ||
+      (control.algorithm != HFPS_FGMRES && control.recycle != HFPS_RECYCLE_NONE) ||
+      !((control.algorithm == HFPS_PCG && control.restart == 0 &&
+         (policy_.unit_linear || policy_.preconditioner == HFPS_PRECONDITIONER_IC0)) ||
+        (control.algorithm == HFPS_BICGSTAB && control.restart == 0 &&
+         policy_.preconditioner == HFPS_PRECONDITIONER_IC0) ||
         (control.algorithm == HFPS_FGMRES && control.restart >= 1 &&
          control.restart <= static_cast<uint32_t>(kMaxFgmresRestart))))
     return fail(HFPS_INVALID_PLAN, kDetailPlan, "invalid solve control");
@@ -1472,8 +1743,9 @@ Status Solver::solve(const double* rhs, double* solution, int memory,
   if (st) st = copy_in(kx_, solution, n, memory);
   if (!st) return st;
   launches_ = 0;
-  st = control.algorithm == HFPS_FGMRES ? krylov_fgmres(control, result, history, capacity)
-                                        : krylov_pcg(control, result, history, capacity);
+  st = control.algorithm == HFPS_FGMRES     ? krylov_fgmres(control, result, history, capacity)
+       : control.algorithm == HFPS_BICGSTAB ? krylov_bicgstab(control, result, history, capacity)
+                                            : krylov_pcg(control, result, history, capacity);
   result.kernel_launches = launches_;
   if (st) {
     st = copy_out(solution, kx_, n, memory);
@@ -1504,7 +1776,7 @@ Status Solver::apply_preconditioner(const double* r, double* z, int memory,
   if (!st) return st;
   st = check(cudaMemsetAsync(d_scalars_, 0, sizeof(Scalars), stream_), "scalars");
   if (!st) return st;
-  st = mg_apply(precision == HFPS_MIXED);
+  st = precondition(precision == HFPS_MIXED);
   if (!st) return st;
   st = copy_out(z, kz_, n, memory);
   if (!st) return st;

@@ -94,6 +94,12 @@ class Solver {
                          double* dst);
   // The MG preconditioner: z = M r on the internal r/z buffers.
   Status mg_apply(bool mixed);
+  // z = M r on kr_/kz_ with the policy's preconditioner (MG or cold IC(0)).
+  Status precondition(bool mixed);
+  Status dic_apply();
+  Status dic_factor();
+  Status krylov_bicgstab(const hfps_control& control, hfps_result& result,
+                         double* history, uint32_t capacity);
   template <class T>
   void mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
                   double* z);
@@ -176,6 +182,12 @@ class Solver {
   double* rc_image_[kRecycleMax]{};   // projection scratch: A d_i
   bool rc_capture_{}, rc_guard_only_{}, rc_cycle_active_{}, rc_pending_{};
   int rc_count_{}, rc_oldest_{};
+  // Cold-path IC(0): decorated row diagonals and inverse pivots (level 0),
+  // and the captured wavefront apply (kr_ -> kz_).
+  double* dic_rows_{};
+  double* dic_inv_{};
+  cudaGraphExec_t dic_graph_{};
+  size_t dic_nodes_{};
   cudaGraphExec_t mg_graph_[2]{};
   size_t mg_nodes_[2]{};      // kernels per MG application (graph nodes)
   uint64_t launches_{};       // kernels launched since the last reset

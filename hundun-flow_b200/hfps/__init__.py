@@ -6,5 +6,5 @@ of include/hf_pressure_solver.h; this package is its thin Python mirror
 and a torch.autograd wrapper used for gradient checks (``autograd``).
 """
 from . import workloads  # noqa: F401
-from .solver import (DEVICE, FGMRES, FP64, HOST, MIXED, PCG, Policy,  # noqa: F401
-                     PressureSolver, SolveOptions, SolverError, library_path)
+from .solver import (BICGSTAB, DEVICE, FGMRES, FP64, HOST, IC0, MG, MIXED, PCG,  # noqa: F401
+                     Policy, PressureSolver, SolveOptions, SolverError, library_path)

@@ -24,7 +24,8 @@ LIBRARY = os.path.join(PACKAGE, "libhfps.so")
 
 HOST, DEVICE = 0, 1
 FP64, MIXED = 0, 1
-PCG, FGMRES = 0, 1
+PCG, FGMRES, BICGSTAB = 0, 1, 2
+MG, IC0 = 0, 1
 RECYCLE = {"none": 0, "capture": 1, "project": 2, "guard": 3}
 
 STATUS = ["ok", "invalid_case", "invalid_plan", "allocation_failure", "mpi_failure",
@@ -51,7 +52,8 @@ class Policy(ctypes.Structure):
                 ("minimum_coarse_extent", ctypes.c_int), ("unit_linear", ctypes.c_int),
                 ("chebyshev_lower_spectrum_fraction", ctypes.c_double),
                 ("anisotropy_threshold", ctypes.c_double),
-                ("diagonal_shortcut_maximum_ratio", ctypes.c_double)]
+                ("diagonal_shortcut_maximum_ratio", ctypes.c_double),
+                ("preconditioner", ctypes.c_int)]
 
     @staticmethod
     def default() -> "Policy":

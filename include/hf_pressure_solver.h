@@ -68,7 +68,16 @@ typedef enum hfps_boundary {
 typedef enum hfps_memory { HFPS_HOST = 0, HFPS_DEVICE = 1 } hfps_memory;
 
 /* LinearAlgorithm (include/hundun/v04_case.hpp:21). */
-typedef enum hfps_algorithm { HFPS_PCG = 0, HFPS_FGMRES = 1 } hfps_algorithm;
+typedef enum hfps_algorithm { HFPS_PCG = 0, HFPS_FGMRES = 1, HFPS_BICGSTAB = 2 } hfps_algorithm;
+
+/* Preconditioner: the multigrid plan, or the cold path's diagonal IC(0)
+ * (ColdPressureIccg, src/solver_iccg.hpp:224-293; ColdPressureDilu,
+ * src/solver_cold.hpp:484-560, the same factorisation on the symmetric
+ * pressure rows), evaluated in the reference's lexicographic order. */
+typedef enum hfps_preconditioner {
+  HFPS_PRECONDITIONER_MG = 0,
+  HFPS_PRECONDITIONER_IC0 = 1
+} hfps_preconditioner;
 
 /* FP64: every kernel in FP64.  MIXED: MG hierarchy stored and cycled in
  * FP32 inside an FP64 Krylov/refinement loop; residuals, dot products, norms
@@ -90,6 +99,7 @@ typedef struct hfps_policy {
   double chebyshev_lower_spectrum_fraction; /* default 0.3 */
   double anisotropy_threshold;              /* default 4.0 */
   double diagonal_shortcut_maximum_ratio;   /* default 0.0 (off) */
+  int preconditioner;                       /* hfps_preconditioner, default MG */
 } hfps_policy;
 
 /* Cartesian geometry: face coordinates per axis (n+1 values each),

@@ -135,7 +135,7 @@ def main():
             ref = ref_oracle.RefSession(system, ref_oracle.MgPolicy(**pol), algorithm=algorithm,
                                         preconditioner=pc)
             cold_arrays[f"{name}_{pc}_apply"] = ref.apply_cold(v)
-            x, info = ref.solve(system.rhs, rtol=1e-10, maxit=4000)
+            x, info = ref.solve(system.rhs, rtol=1e-12, maxit=8000)
             ref.close()
             cold_arrays[f"{name}_{algorithm}_{pc}_x"] = x
             entry[f"{algorithm}_{pc}"] = {"iterations": info["iterations"],

@@ -281,7 +281,7 @@ def test_cold_path_restatement_reproduces_reference_golden(name):
     assert np.array_equal(z, gold[f"{name}_iccg_apply"])
     assert np.array_equal(z, gold[f"{name}_dilu_apply"])
     for algorithm, pc in (("pcg", "iccg"), ("bicgstab", "dilu")):
-        x, info = o.solve(s.rhs, rtol=1e-10, maxit=4000, algorithm=algorithm)
+        x, info = o.solve(s.rhs, rtol=1e-12, maxit=8000, algorithm=algorithm)
         assert info["iterations"] == meta[f"{algorithm}_{pc}"]["iterations"]
         assert info["operator_applies"] == meta[f"{algorithm}_{pc}"]["operator_applies"]
         assert np.array_equal(x, gold[f"{name}_{algorithm}_{pc}_x"])
