@@ -28,6 +28,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "hundun-flow_b200"))
 
@@ -50,6 +52,9 @@ def parse():
                    help="override the grid (testing only; the bench line is the 256^3 case)")
     p.add_argument("--single", choices=["fp64", "mixed"], default=None,
                    help="profiling aid: one warm-up solve, then one solve, no timing/JSON")
+    p.add_argument("--config", choices=["three_spheres512"], default=None,
+                   help="the 512^3 three-sphere mixed forward + adjoint sequence "
+                        "(its own JSON line; not the headline metric)")
     return p.parse_args()
 
 
@@ -480,11 +485,98 @@ def run_single(args):
     solver.close()
 
 
+def run_three_spheres(args):
+    """512^3 spherical flame with three IBM spheres: `steps` warm-started
+    mixed-precision forward solves, each followed by a mixed adjoint solve of
+    L = 0.5 sum_fluid (p - p_t)^2 (p_t from seed 7), with size-independent
+    checks: the forward true residual, the adjoint identity lambda.b =
+    (dL/dp).p (A is symmetric), the mixed solution against an FP64 solve, and
+    the device memory in use."""
+    import torch
+    import hfps
+    from hfps import workloads
+    device = torch.device("cuda", 0)
+    free0, total = torch.cuda.mem_get_info(device)
+    system = workloads.make("three_spheres512")
+    solver = hfps.PressureSolver.from_system(system, hfps.Policy.production(),
+                                             stream=torch.cuda.current_stream(device))
+    n = system.cells
+    rhs0 = torch.from_numpy(system.rhs.reshape(-1)).to(device)
+    active = torch.from_numpy(system.active.reshape(-1).astype(np.bool_)).to(device)
+    target = workloads.normals_torch(7, n, device=device)
+    opts = hfps.SolveOptions(rtol=RTOL, maxit=400, precision=hfps.MIXED)
+    x = torch.zeros(n, dtype=torch.float64, device=device)
+    solver.solve(rhs0, x0=x.clone(), options=opts, history=False)  # warm-up, graphs
+    forward_ms, adjoint_ms, iters, adj_iters, identity, residuals = [], [], [], [], [], []
+    start = torch.cuda.Event(enable_timing=True)
+    mid = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    free1, _ = torch.cuda.mem_get_info(device)
+    for k in range(args.steps):
+        rhs = rhs0 + workloads.flux_divergence_rhs_torch(1 + k, system.faces, system.boundary,
+                                                         system.active, 0.05, device=device)
+        x_start = x.clone()
+        torch.cuda.synchronize()
+        start.record()
+        x, info = solver.solve(rhs, x0=x, out=x, options=opts, history=False)
+        mid.record()
+        dl_dp = torch.where(active, x - target, torch.zeros_like(x))
+        lam, grads, ainfo = solver.adjoint(x, dl_dp, options=opts)
+        stop.record()
+        torch.cuda.synchronize()
+        forward_ms.append(start.elapsed_time(mid))
+        adjoint_ms.append(mid.elapsed_time(stop))
+        iters.append(info["iterations"])
+        adj_iters.append(ainfo["iterations"])
+        residuals.append(info["final_true_residual"] / info["rhs_norm"])
+        lb = float(torch.dot(lam, torch.where(active, rhs, torch.zeros_like(rhs))))
+        gp = float(torch.dot(dl_dp, x))
+        identity.append(abs(lb - gp) / max(abs(gp), 1e-300))
+    # The plain FP64 GPU forward solve of the last step (same rhs, same warm
+    # start), and the FP64 adjoint of the mixed solution's loss: the gradient
+    # errors compare the mixed adjoint (lambda and every face gradient) with it.
+    torch.cuda.synchronize()
+    start.record()
+    x64, i64 = solver.solve(rhs, x0=x_start, rtol=RTOL, maxit=400, history=False)
+    stop.record()
+    torch.cuda.synchronize()
+    fp64_ms = start.elapsed_time(stop)
+    mixed_error = float(torch.linalg.vector_norm(x - x64) / torch.linalg.vector_norm(x64))
+    lam64, grads64, _ = solver.adjoint(x, dl_dp, rtol=RTOL, maxit=400)
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+    lambda_error = rel(lam, lam64)
+    face_error = max(rel(g, g64) for g, g64 in zip(grads, grads64))
+    ms, nbytes = solver.profile_kernel("smooth_fp32", 10)
+    line = {
+        "config": {"workload": "three_spheres512 (512^3 spherical flame, three IBM spheres)",
+                   "cells": n, "sequence": args.steps,
+                   "algorithm": "mixed MG-PCG forward + mixed adjoint per step"},
+        "forward_ms": statistics.mean(forward_ms), "adjoint_ms": statistics.mean(adjoint_ms),
+        "forward_iterations": iters, "adjoint_iterations": adj_iters,
+        "max_relative_true_residual": max(residuals),
+        "max_adjoint_identity_error": max(identity),
+        "mixed_vs_fp64_relative_error": mixed_error, "fp64_iterations": i64["iterations"],
+        "fp64_forward_ms": fp64_ms,
+        "adjoint_lambda_vs_fp64_relative_error": lambda_error,
+        "adjoint_face_gradient_vs_fp64_relative_error": face_error,
+        "level0_smoother_fp32_gbs": nbytes / (ms * 1e-3) / 1e9 if ms else None,
+        "device_memory_gb": (free0 - free1) / 1e9, "device_total_gb": total / 1e9,
+    }
+    print(json.dumps(line), flush=True)
+    solver.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     if args.single:
         run_single(args)
+        return
+    if args.config == "three_spheres512":
+        run_three_spheres(args)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -185,7 +185,11 @@ Status Solver::create(const hfps_geometry& g, const hfps_policy& policy,
     }
   }
   if (stream == nullptr) {
-    Status st = s->check(cudaStreamCreateWithFlags(&s->stream_, cudaStreamNonBlocking),
+    // A blocking stream: work the caller queued on the legacy default stream
+    // (device inputs it produced there, a zero-filled initial guess) is
+    // ordered before the solver's copies, and the caller's later work there
+    // after them.  A non-blocking stream would race with both.
+    Status st = s->check(cudaStreamCreateWithFlags(&s->stream_, cudaStreamDefault),
                          "stream create");
     if (!st) {
       error = s->error_;

@@ -179,8 +179,11 @@ HFPS_API void hfps_default_control(hfps_control* control);
 /* Builds the level hierarchy and workspaces on the current CUDA device.
  * Replaces NativeCartesianMgPlan::compile + make_mg_workspace_requirements +
  * SolverWorkspace::bind (include/hundun/v04_linear.hpp:945-960, 1046-1064).
- * `stream` is a cudaStream_t; NULL makes the solver create and own a
- * non-blocking stream of its own. */
+ * `stream` is a cudaStream_t on which every later call reads its device
+ * inputs and writes its device outputs; the caller orders the producers of
+ * HFPS_DEVICE inputs before the call on that stream.  NULL (also what a
+ * caller on the legacy default stream passes) makes the solver create and
+ * own a blocking stream, which is ordered with the legacy default stream. */
 HFPS_API int hfps_create(const hfps_geometry* geometry, const hfps_policy* policy,
                 void* stream, hfps_solver** out);
 
