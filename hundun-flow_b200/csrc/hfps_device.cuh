@@ -94,18 +94,38 @@ __device__ __forceinline__ int face_y_index(const Level<T>& L, int c, int k) {
   return c + L.nx * k;
 }
 
+// How a shared device body reads a vector: an ordinary load, or the
+// read-only data path (ld.global.nc) for arrays no thread writes during the
+// launch.
+struct PlainLoad {
+  template <class T>
+  __device__ __forceinline__ static T get(const T* p) { return *p; }
+};
+struct RoLoad {
+  template <class T>
+  __device__ __forceinline__ static T get(const T* p) { return __ldg(p); }
+};
+
+__device__ __forceinline__ void cell_coords(int c, int nx, int ny, int& i,
+                                            int& j, int& k) {
+  const int row = c / nx;
+  i = c - row * nx;
+  k = row / ny;
+  j = row - k * ny;
+}
+
 // A x at one cell, in the reference's accumulation order.
-template <class T>
+template <class T, class Ld = PlainLoad>
 __device__ __forceinline__ T row_value(const Level<T>& L, const T* x, int i,
                                        int j, int k, int c) {
   const int plane = L.nx * L.ny;
-  const T xc = x[c];
-  const T xm = i > 0 ? x[c - 1] : ((L.neumann & 1u) ? xc : T(0));
-  const T xp = i + 1 < L.nx ? x[c + 1] : ((L.neumann & 2u) ? xc : T(0));
-  const T ym = j > 0 ? x[c - L.nx] : ((L.neumann & 4u) ? xc : T(0));
-  const T yp = j + 1 < L.ny ? x[c + L.nx] : ((L.neumann & 8u) ? xc : T(0));
-  const T zm = k > 0 ? x[c - plane] : ((L.neumann & 16u) ? xc : T(0));
-  const T zp = k + 1 < L.nz ? x[c + plane] : ((L.neumann & 32u) ? xc : T(0));
+  const T xc = Ld::get(x + c);
+  const T xm = i > 0 ? Ld::get(x + c - 1) : ((L.neumann & 1u) ? xc : T(0));
+  const T xp = i + 1 < L.nx ? Ld::get(x + c + 1) : ((L.neumann & 2u) ? xc : T(0));
+  const T ym = j > 0 ? Ld::get(x + c - L.nx) : ((L.neumann & 4u) ? xc : T(0));
+  const T yp = j + 1 < L.ny ? Ld::get(x + c + L.nx) : ((L.neumann & 8u) ? xc : T(0));
+  const T zm = k > 0 ? Ld::get(x + c - plane) : ((L.neumann & 16u) ? xc : T(0));
+  const T zp = k + 1 < L.nz ? Ld::get(x + c + plane) : ((L.neumann & 32u) ? xc : T(0));
   const int fxi = face_x_index(L, c, j, k);
   const int fyi = face_y_index(L, c, k);
   T v = L.diag[c] * xc;
@@ -122,21 +142,23 @@ __device__ __forceinline__ T row_value(const Level<T>& L, const T* x, int i,
 // transverse and end terms (level_neighbor, src/solver_mg.cpp:2222-2262).
 // x may live in shared memory that other threads update between barriers
 // (coarsest-level kernels), so it is not __restrict__-qualified.
-template <class T>
+template <class T, class Ld = PlainLoad>
 __device__ __forceinline__ T line_neighbour(const Level<T>& L, const T* x,
                                             int i, int j, int k, int c,
                                             int axis, int dir) {
   if (axis == 0) {
-    if (dir < 0) return i > 0 ? x[c - 1] : ((L.neumann & 1u) ? x[c] : T(0));
-    return i + 1 < L.nx ? x[c + 1] : ((L.neumann & 2u) ? x[c] : T(0));
+    if (dir < 0) return i > 0 ? Ld::get(x + c - 1) : ((L.neumann & 1u) ? Ld::get(x + c) : T(0));
+    return i + 1 < L.nx ? Ld::get(x + c + 1) : ((L.neumann & 2u) ? Ld::get(x + c) : T(0));
   }
   if (axis == 1) {
-    if (dir < 0) return j > 0 ? x[c - L.nx] : ((L.neumann & 4u) ? x[c] : T(0));
-    return j + 1 < L.ny ? x[c + L.nx] : ((L.neumann & 8u) ? x[c] : T(0));
+    if (dir < 0)
+      return j > 0 ? Ld::get(x + c - L.nx) : ((L.neumann & 4u) ? Ld::get(x + c) : T(0));
+    return j + 1 < L.ny ? Ld::get(x + c + L.nx) : ((L.neumann & 8u) ? Ld::get(x + c) : T(0));
   }
   const int plane = L.nx * L.ny;
-  if (dir < 0) return k > 0 ? x[c - plane] : ((L.neumann & 16u) ? x[c] : T(0));
-  return k + 1 < L.nz ? x[c + plane] : ((L.neumann & 32u) ? x[c] : T(0));
+  if (dir < 0)
+    return k > 0 ? Ld::get(x + c - plane) : ((L.neumann & 16u) ? Ld::get(x + c) : T(0));
+  return k + 1 < L.nz ? Ld::get(x + c + plane) : ((L.neumann & 32u) ? Ld::get(x + c) : T(0));
 }
 
 // Row s of the line system through cell (fa, fb) along `axis`: the same

@@ -9,6 +9,7 @@
 // block pass, finished by the last block to arrive (fixed order, so every
 // sum is reproducible run to run).
 #include "kernels.hpp"
+#include "phase_device.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -95,14 +96,6 @@ __device__ void apply_scalar_op(Scalars* sc, int op, double sum) {
   }
 }
 
-__device__ __forceinline__ void cell_coords(int c, int nx, int ny, int& i,
-                                            int& j, int& k) {
-  const int row = c / nx;
-  i = c - row * nx;
-  k = row / ny;
-  j = row - k * ny;
-}
-
 // ---------------------------------------------------------------------------
 // Level operators: apply_level_matrix / apply_level_defect
 // (src/solver_mg.cpp:2569-2767).
@@ -142,19 +135,9 @@ __global__ void k_rb_color(Level<T> L, T* __restrict__ x,
   grid_dependency_sync();
   const int hx = (L.nx + 1) >> 1;
   const int n = hx * L.ny * L.nz;
-  const T omega = T(0.72);
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n;
-       t += gridDim.x * blockDim.x) {
-    const int row = t / hx;
-    const int ih = t - row * hx;
-    const int k = row / L.ny;
-    const int j = row - k * L.ny;
-    const int i = 2 * ih + ((j + k + color) & 1);
-    if (i >= L.nx) continue;
-    const int c = i + L.nx * row;
-    const T value = row_value(L, x, i, j, k, c);
-    x[c] += omega * (b[c] - value) / L.diag[c];
-  }
+       t += gridDim.x * blockDim.x)
+    rb_slot<T>(L, x, b, color, t);
 }
 
 // One Chebyshev-Jacobi stage (chebyshev_stream_bulk_kernel,
@@ -168,16 +151,8 @@ __global__ void k_chebyshev_stage(Level<T> L, const T* __restrict__ x,
   grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
-    int i, j, k;
-    cell_coords(c, L.nx, L.ny, i, j, k);
-    const T value = row_value(L, x, i, j, k, c);
-    const T defect = b[c] - value;
-    const T scaled = residual_factor * defect / L.diag[c];
-    const T d = first ? scaled : previous_factor * direction[c] + scaled;
-    direction[c] = d;
-    next[c] = x[c] + d;
-  }
+       c += gridDim.x * blockDim.x)
+    chebyshev_cell<T>(L, x, b, direction, next, previous_factor, residual_factor, first, c);
 }
 
 // Thomas solve of one line (solve_one, src/solver_mg.cpp:3388-3493).
@@ -255,22 +230,9 @@ __global__ void k_defect_restrict(Level<T> F, const T* __restrict__ x,
                                   int mask) {
   grid_dependency_sync();
   const int n = C.nx * C.ny * C.nz;
-  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
   for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
        cc += gridDim.x * blockDim.x) {
-    int ci, cj, ck;
-    cell_coords(cc, C.nx, C.ny, ci, cj, ck);
-    const int xb = mx ? 2 * ci : ci, yb = my ? 2 * cj : cj, zb = mz ? 2 * ck : ck;
-    T sum = T(0);
-    for (int dz = 0; dz <= mz; ++dz)
-      for (int dy = 0; dy <= my; ++dy)
-        for (int dx = 0; dx <= mx; ++dx) {
-          const int fi = xb + dx, fj = yb + dy, fk = zb + dz;
-          if (fi >= F.nx || fj >= F.ny || fk >= F.nz) continue;
-          const int fc = fi + F.nx * (fj + F.ny * fk);
-          sum += b[fc] - row_value(F, x, fi, fj, fk, fc);
-        }
-    cb[cc] = sum;
+    cb[cc] = defect_restrict_cell<T>(F, x, b, C, mask, cc);
     cx[cc] = T(0);
   }
 }
@@ -299,42 +261,9 @@ __global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
   }
 }
 
-__device__ __forceinline__ void interp_axis(int fine, int coarsened,
-                                            int extent, int& left, int& right,
-                                            double& weight) {
-  if (!coarsened) {
-    left = right = fine;
-    weight = 0.0;
-    return;
-  }
-  const int parent = fine >> 1;
-  if ((fine & 1) == 0) {
-    left = parent - 1;
-    right = parent;
-    weight = 0.75;
-  } else {
-    left = parent;
-    right = parent + 1;
-    weight = 0.25;
-  }
-  if (left < 0) {
-    left = right = 0;
-    weight = 0.0;
-  } else if (right >= extent) {
-    left = right = extent - 1;
-    weight = 0.0;
-  }
-}
-
-// Trilinear prolongation and add, zero on solid cells (prolongate_add,
-// src/solver_mg.cpp:3893-3994).  Weights are formed in double exactly as
-// the reference does and rounded once to T for the FP32 hierarchy.
-//
-// One fine cell per thread, branch-free: the up to 2x2x2 coarse candidates
-// are loaded unconditionally (a degenerate axis repeats its one index) and
-// the terms are added in the reference's order (z outer, x inner) with the
-// absent ones skipped by selects, so the sum is the reference's bit for bit
-// while all loads of a cell are in flight together.
+// Trilinear prolongation and add, zero on solid cells (prolongate_cell):
+// one fine cell per thread, the coarse correction through the read-only
+// path.
 template <class T>
 __global__ void k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C,
                              const T* __restrict__ cx, int mask) {
@@ -342,42 +271,7 @@ __global__ void k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C,
   const int n = F.nx * F.ny * F.nz;
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
-  const bool fluid = F.fluid[c] != 0;
-  const T old = x[c];
-  int i, j, k;
-  cell_coords(c, F.nx, F.ny, i, j, k);
-  int xi[2], yi[2], zi[2];
-  double xw, yw, zw;
-  interp_axis(i, mx, C.nx, xi[0], xi[1], xw);
-  interp_axis(j, my, C.ny, yi[0], yi[1], yw);
-  interp_axis(k, mz, C.nz, zi[0], zi[1], zw);
-  const bool two_x = xi[0] != xi[1], two_y = yi[0] != yi[1], two_z = zi[0] != zi[1];
-  T term[2][2][2];
-#pragma unroll
-  for (int az = 0; az < 2; ++az)
-#pragma unroll
-    for (int ay = 0; ay < 2; ++ay)
-#pragma unroll
-      for (int ax = 0; ax < 2; ++ax) {
-        const double wz = az == 0 ? 1.0 - zw : zw;
-        const double wy = ay == 0 ? 1.0 - yw : yw;
-        const double wx = ax == 0 ? 1.0 - xw : xw;
-        const T w = static_cast<T>(wx * wy * wz);
-        term[az][ay][ax] = w * __ldg(cx + xi[ax] + C.nx * (yi[ay] + C.ny * zi[az]));
-      }
-  T value = T(0);
-#pragma unroll
-  for (int az = 0; az < 2; ++az)
-#pragma unroll
-    for (int ay = 0; ay < 2; ++ay)
-#pragma unroll
-      for (int ax = 0; ax < 2; ++ax) {
-        const bool on = (az == 0 || two_z) && (ay == 0 || two_y) && (ax == 0 || two_x);
-        const T sum = value + term[az][ay][ax];
-        value = on ? sum : value;
-      }
-  x[c] = fluid ? old + value : T(0);
+  x[c] = prolongate_cell<T, PlainLoad, RoLoad>(F, x, C, cx, mask, c);
 }
 
 // Coarsest level: `sweeps` smoother sweeps in one CTA (mg_cycle coarse
@@ -403,25 +297,7 @@ __global__ void k_coarse_solve(Level<TC> L, T* x, const T* b, TC* xs, TC* bs,
     bw = reinterpret_cast<const TC*>(b);
   }
   if (line_axis < 0) {
-    const TC omega = TC(0.72);
-    const int hx = (L.nx + 1) >> 1;
-    const int half = hx * L.ny * L.nz;
-    for (int s = 0; s < sweeps; ++s) {
-      for (int color = 0; color < 2; ++color) {
-        for (int t = threadIdx.x; t < half; t += blockDim.x) {
-          const int row = t / hx;
-          const int ih = t - row * hx;
-          const int k = row / L.ny;
-          const int j = row - k * L.ny;
-          const int i = 2 * ih + ((j + k + color) & 1);
-          if (i >= L.nx) continue;
-          const int c = i + L.nx * row;
-          const TC value = row_value(L, xw, i, j, k, c);
-          xw[c] += omega * (bw[c] - value) / L.diag[c];
-        }
-        __syncthreads();
-      }
-    }
+    coarse_point_sweeps(L, xw, bw, sweeps, threadIdx.x, blockDim.x);
   } else {
     const int a_extent = line_axis == 0 ? L.ny : L.nx;
     const int b_extent = line_axis == 2 ? L.ny : L.nz;

@@ -102,11 +102,12 @@ template <class T, class TC>
 bool launch_coarse_line(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
                         const TC* fac, int sweeps, int axis, bool columns = false);
 // out = P x + M b with the dense coarsest-level map built by the columns
-// mode above (n <= kCoarseDenseMaxCells; out must not alias x or b).
+// mode above (n <= kCoarseDenseMaxCells; out must not alias x or b).  With
+// x_zero (x is known to be zero) the P half is not read.
 constexpr int kCoarseDenseMaxCells = 2048;
 template <class T>
 void launch_coarse_dense(cudaStream_t s, int n, const double* op, const T* x,
-                         const T* b, T* out);
+                         const T* b, T* out, bool x_zero);
 
 // Coarsest level: `sweeps` smoother sweeps in one CTA, arithmetic in TC.
 // Line mode when line_axis >= 0 (zebra line Gauss-Seidel).

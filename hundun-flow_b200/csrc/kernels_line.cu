@@ -18,92 +18,13 @@
 //   * the coarsest level keeps x and rhs in shared memory for all of its
 //     coarse sweeps in one launch.
 #include "kernels.hpp"
+#include "phase_device.cuh"
 
 #include <algorithm>
 
 namespace hfps {
 namespace {
 
-
-__host__ __device__ __forceinline__ int line_extent(int axis, int nx, int ny,
-                                                    int nz) {
-  return axis == 0 ? nx : (axis == 1 ? ny : nz);
-}
-
-// Cells of one line: c = base + s * stride.
-template <class T>
-__device__ __forceinline__ void line_geometry(const Level<T>& L, int axis,
-                                              int fa, int fb, int& base,
-                                              int& stride) {
-  if (axis == 0) {
-    base = L.nx * (fa + L.ny * fb);
-    stride = 1;
-  } else if (axis == 1) {
-    base = fa + L.nx * L.ny * fb;
-    stride = L.nx;
-  } else {
-    base = fa + L.nx * fb;
-    stride = L.nx * L.ny;
-  }
-}
-
-// The line's own off-diagonal faces at cell c (row s).
-template <class T>
-__device__ __forceinline__ void line_faces(const Level<T>& L, int axis, int c,
-                                           int j, int k, T& lowf, T& highf) {
-  if (axis == 0) {
-    const int f = face_x_index(L, c, j, k);
-    lowf = L.fx[f];
-    highf = L.fx[f + 1];
-  } else if (axis == 1) {
-    const int f = face_y_index(L, c, k);
-    lowf = L.fy[f];
-    highf = L.fy[f + L.nx];
-  } else {
-    lowf = L.fz[c];
-    highf = L.fz[c + L.nx * L.ny];
-  }
-}
-
-__device__ __forceinline__ void line_cell(int axis, int fa, int fb, int s,
-                                          int& i, int& j, int& k) {
-  i = axis == 0 ? s : fa;
-  j = axis == 0 ? fa : (axis == 1 ? s : fb);
-  k = axis == 2 ? s : fb;
-}
-
-// Right-hand side of row s of a line: rhs plus the transverse neighbours and
-// the line-end boundary terms, in the reference's order (line_row's d).
-template <class T, int AXIS>
-__device__ __forceinline__ T line_rhs(const Level<T>& L, const T* x,
-                                      const T* rhs, int fa, int fb, int s,
-                                      int extent, int c) {
-  int i, j, k;
-  line_cell(AXIS, fa, fb, s, i, j, k);
-  const int plane = L.nx * L.ny;
-  const int fxi = face_x_index(L, c, j, k);
-  const int fyi = face_y_index(L, c, k);
-  T d = rhs[c];
-  if (AXIS != 0) {
-    d += L.fx[fxi] * line_neighbour(L, x, i, j, k, c, 0, -1);
-    d += L.fx[fxi + 1] * line_neighbour(L, x, i, j, k, c, 0, 1);
-  }
-  if (AXIS != 1) {
-    d += L.fy[fyi] * line_neighbour(L, x, i, j, k, c, 1, -1);
-    d += L.fy[fyi + L.nx] * line_neighbour(L, x, i, j, k, c, 1, 1);
-  }
-  if (AXIS != 2) {
-    d += L.fz[c] * line_neighbour(L, x, i, j, k, c, 2, -1);
-    d += L.fz[c + plane] * line_neighbour(L, x, i, j, k, c, 2, 1);
-  }
-  if (s == 0 || s + 1 == extent) {
-    T lowf, highf;
-    line_faces(L, AXIS, c, j, k, lowf, highf);
-    if (s == 0) d += lowf * line_neighbour(L, x, i, j, k, c, AXIS, -1);
-    if (s + 1 == extent) d += highf * line_neighbour(L, x, i, j, k, c, AXIS, 1);
-  }
-  return d;
-}
 
 // Right-hand side of the rows of one line with everything that is constant
 // along the line hoisted: the transverse neighbours' offsets (0 where the
@@ -458,48 +379,6 @@ __global__ void __launch_bounds__(1024) k_pcr_factors(Level<T> L, int axis, int 
   if (valid) fac[(2 * step) * slab + at] = sb[s];
 }
 
-// Factors of one row (2*STEPS multipliers + final diagonal) in registers.
-template <class T, int STEPS>
-struct PcrRow {
-  T k[2 * STEPS + 1];
-};
-
-template <class T, int STEPS>
-__device__ __forceinline__ void pcr_load(const T* __restrict__ fac, size_t slab,
-                                         size_t at, PcrRow<T, STEPS>& r) {
-#pragma unroll
-  for (int e = 0; e <= 2 * STEPS; ++e) r.k[e] = fac[e * slab + at];
-}
-
-// PCR right-hand-side elimination with register-held factors; returns x_s.
-// sd is written by the other threads of the line between barriers, so it
-// must not be __restrict__-qualified.
-template <class T, int STEPS>
-__device__ __forceinline__ T pcr_apply(const PcrRow<T, STEPS>& r, T* sd, int s) {
-  constexpr int P = 1 << STEPS;
-#pragma unroll
-  for (int step = 0; step < STEPS; ++step) {
-    const int h = 1 << step;
-    const int lo = s - h, hi = s + h;
-    const T dlo = lo >= 0 ? sd[lo] : T(0);
-    const T dhi = hi < P ? sd[hi] : T(0);
-    const T nd = sd[s] - dlo * r.k[2 * step] - dhi * r.k[2 * step + 1];
-    __syncthreads();
-    sd[s] = nd;
-    __syncthreads();
-  }
-  return sd[s] / r.k[2 * STEPS];
-}
-
-template <class T>
-__device__ __forceinline__ T line_rhs_any(const Level<T>& L, const T* x,
-                                          const T* rhs, int axis, int fa,
-                                          int fb, int s, int extent, int c) {
-  if (axis == 0) return line_rhs<T, 0>(L, x, rhs, fa, fb, s, extent, c);
-  if (axis == 1) return line_rhs<T, 1>(L, x, rhs, fa, fb, s, extent, c);
-  return line_rhs<T, 2>(L, x, rhs, fa, fb, s, extent, c);
-}
-
 // One zebra colour with PCR: blockDim = (P, lines per block), P = 2^STEPS.
 template <class T, int STEPS>
 __global__ void __launch_bounds__(1024) k_line_pcr_factored_color(Level<T> L, T* __restrict__ x,
@@ -507,34 +386,10 @@ __global__ void __launch_bounds__(1024) k_line_pcr_factored_color(Level<T> L, T*
                                           const T* __restrict__ fac, int axis,
                                           int color) {
   grid_dependency_sync();
-  constexpr int P = 1 << STEPS;
   extern __shared__ unsigned char pcr_rhs_smem[];
-  T* sd = reinterpret_cast<T*>(pcr_rhs_smem) + threadIdx.y * P;
-  const int a_extent = axis == 0 ? L.ny : L.nx;
-  const int b_extent = axis == 2 ? L.ny : L.nz;
-  const int ha = (a_extent + 1) >> 1;
-  const int extent = line_extent(axis, L.nx, L.ny, L.nz);
-  const int t = blockIdx.x * blockDim.y + threadIdx.y;
-  const int fb = t / ha;
-  const int fa = 2 * (t - fb * ha) + ((fb + color) & 1);
-  const bool valid = t < ha * b_extent && fa < a_extent;
-  const int s = threadIdx.x;
-  const size_t slab = static_cast<size_t>(a_extent) * b_extent * P;
-  const size_t at = static_cast<size_t>(valid ? fa + a_extent * fb : 0) * P + s;
-  PcrRow<T, STEPS> r;
-  pcr_load(fac, slab, at, r);
-  int c = 0;
-  T d = T(0);
-  if (valid && s < extent) {
-    int i, j, k;
-    line_cell(axis, fa, fb, s, i, j, k);
-    c = i + L.nx * (j + L.ny * k);
-    d = line_rhs_any(L, x, rhs, axis, fa, fb, s, extent, c);
-  }
-  sd[s] = d;
-  __syncthreads();
-  const T value = pcr_apply(r, sd, s);
-  if (valid && s < extent) x[c] = value;
+  T* sd = reinterpret_cast<T*>(pcr_rhs_smem) + threadIdx.y * (1 << STEPS);
+  pcr_line_slot<T, STEPS>(L, x, rhs, fac, axis, color, blockIdx.x * blockDim.y + threadIdx.y,
+                          threadIdx.x, sd);
 }
 
 // One zebra colour pass of the coarsest-level kernel for the lines handled
@@ -820,60 +675,38 @@ template bool launch_coarse_line<float, double>(cudaStream_t, const Level<double
 // columns mode of k_coarse_line_smem writes them.  A block owns 32 rows (one
 // per lane); its 32 warps take every 32nd column with 8 column loads in
 // flight per thread, and the 32 partial sums of a row are added in warp
-// order, so the result is reproducible.
-constexpr int kDenseWarps = 32;
-constexpr int kDenseUnroll = 8;
-
+// order, so the result is reproducible (dense_rows).
 template <class T>
 __global__ void __launch_bounds__(32 * kDenseWarps)
     k_coarse_dense(int n, const double* __restrict__ op, const T* __restrict__ x,
-                   const T* __restrict__ b, T* __restrict__ out) {
+                   const T* __restrict__ b, T* __restrict__ out, bool x_zero) {
   grid_dependency_sync();
   extern __shared__ double dense_smem[];
   double* v = dense_smem;                    // [2n]: x then b, widened
   double* part = dense_smem + 2 * n;         // [kDenseWarps][32]
   const int tid = threadIdx.y * 32 + threadIdx.x;
   for (int j = tid; j < n; j += 32 * kDenseWarps) {
-    v[j] = static_cast<double>(x[j]);
+    v[j] = x_zero ? 0.0 : static_cast<double>(x[j]);
     v[n + j] = static_cast<double>(b[j]);
   }
   __syncthreads();
-  const int row = min(blockIdx.x * 32 + threadIdx.x, n - 1);
-  const int cols = 2 * n;
-  double acc = 0.0;
-  for (int j0 = threadIdx.y; j0 < cols; j0 += kDenseWarps * kDenseUnroll) {
-    double m[kDenseUnroll];
-#pragma unroll
-    for (int u = 0; u < kDenseUnroll; ++u) {
-      const int j = min(j0 + u * kDenseWarps, cols - 1);
-      m[u] = __ldg(op + static_cast<size_t>(j) * n + row);
-    }
-#pragma unroll
-    for (int u = 0; u < kDenseUnroll; ++u)
-      if (j0 + u * kDenseWarps < cols) acc += m[u] * v[j0 + u * kDenseWarps];
-  }
-  part[threadIdx.y * 32 + threadIdx.x] = acc;
-  __syncthreads();
-  if (threadIdx.y == 0 && blockIdx.x * 32 + threadIdx.x < n) {
-    double sum = part[threadIdx.x];
-    for (int w = 1; w < kDenseWarps; ++w) sum += part[w * 32 + threadIdx.x];
-    out[blockIdx.x * 32 + threadIdx.x] = static_cast<T>(sum);
-  }
+  dense_rows<T>(n, op, v, part, blockIdx.x, threadIdx.x, threadIdx.y, x_zero, out);
 }
 
 template <class T>
 void launch_coarse_dense(cudaStream_t s, int n, const double* op, const T* x,
-                         const T* b, T* out) {
+                         const T* b, T* out, bool x_zero) {
   const size_t smem = (2 * static_cast<size_t>(n) + 32 * kDenseWarps) * sizeof(double);
   if (smem > 48 * 1024)
     cudaFuncSetAttribute(k_coarse_dense<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
-  launch(k_coarse_dense<T>, (n + 31) / 32, dim3(32, kDenseWarps), smem, s, n, op, x, b, out);
+  launch(k_coarse_dense<T>, (n + 31) / 32, dim3(32, kDenseWarps), smem, s, n, op, x, b, out,
+         x_zero);
 }
 
 template void launch_coarse_dense<double>(cudaStream_t, int, const double*, const double*,
-                                          const double*, double*);
+                                          const double*, double*, bool);
 template void launch_coarse_dense<float>(cudaStream_t, int, const double*, const float*,
-                                         const float*, float*);
+                                         const float*, float*, bool);
 
 }  // namespace hfps

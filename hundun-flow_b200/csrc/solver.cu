@@ -728,7 +728,7 @@ void Solver::smooth(std::vector<DeviceLevel<T>>& levels, int level, int sweeps,
 }
 
 template <class T>
-void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels) {
+void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels, bool x_zero) {
   DeviceLevel<T>& L = levels.back();
   DeviceLevel<double>& D = l64_.back();
   const Level<double> view = D.view(neumann_);
@@ -741,7 +741,7 @@ void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels) {
     return;
   }
   if (coarse_dense_) {
-    launch_coarse_dense<T>(stream_, L.cells(), coarse_op_, L.x, L.b, L.t);
+    launch_coarse_dense<T>(stream_, L.cells(), coarse_op_, L.x, L.b, L.t, x_zero);
     std::swap(L.x, L.t);
     return;
   }
@@ -755,9 +755,10 @@ void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels) {
 }
 
 template <class T>
-void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter) {
+void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter,
+                   bool x_zero) {
   if (level + 1 == static_cast<int>(levels.size())) {
-    coarse_solve(levels);
+    coarse_solve(levels, x_zero);
     return;
   }
   DeviceLevel<T>& F = levels[level];
@@ -766,8 +767,8 @@ void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter) 
   // Retained defect + restrict_residual in one pass.
   launch_defect_restrict<T>(stream_, F.view(neumann_), F.x, F.b, C.view(neumann_),
                             C.b, C.x, F.coarsen_mask);
-  cycle(levels, level + 1, counter);
-  if (counter > 1) cycle(levels, level + 1, counter - 1);
+  cycle(levels, level + 1, counter, true);
+  if (counter > 1) cycle(levels, level + 1, counter - 1, false);
   launch_prolongate<T>(stream_, F.view(neumann_), F.x, C.view(neumann_), C.x,
                        F.coarsen_mask);
   smooth(levels, level, policy_.post_sweeps, true);
@@ -786,7 +787,7 @@ void Solver::mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
   if (diagonal_shortcut_) {
     launch_diagonal_solve<T>(stream_, n, L0.b, L0.diag, L0.x);
   } else {
-    cycle(levels, 0, policy_.cycle == 1 ? 2 : 1);
+    cycle(levels, 0, policy_.cycle == 1 ? 2 : 1, true);
   }
   if (policy_.unit_linear) {
     launch_mg_exit<T>(stream_, n, L0.x, d_active_, nullptr, z);

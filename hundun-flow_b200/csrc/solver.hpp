@@ -104,12 +104,12 @@ class Solver {
   void mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
                   double* z);
   template <class T>
-  void cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter);
+  void cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter, bool x_zero);
   template <class T>
   void smooth(std::vector<DeviceLevel<T>>& levels, int level, int sweeps,
               bool reverse);
   template <class T>
-  void coarse_solve(std::vector<DeviceLevel<T>>& levels);
+  void coarse_solve(std::vector<DeviceLevel<T>>& levels, bool x_zero);
   Status krylov_pcg(const hfps_control& control, hfps_result& result,
                     double* history, uint32_t capacity);
   Status krylov_fgmres(const hfps_control& control, hfps_result& result,
