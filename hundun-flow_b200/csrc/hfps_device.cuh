@@ -114,18 +114,39 @@ __device__ __forceinline__ void cell_coords(int c, int nx, int ny, int& i,
   j = row - k * ny;
 }
 
+// Where a level's vector stores cell (i, j, k) (c = its x-fastest index).
+// NaturalPos: at c.  SplitPos ("split rows", used for the finest level of a
+// y- or z-line hierarchy): every x-row stores its even-i cells and then its
+// odd-i cells, each half hx = (nx + 1) / 2 long, so that one zebra colour
+// of a row is contiguous.
+struct NaturalPos {
+  __device__ __forceinline__ int operator()(int c, int, int, int) const { return c; }
+};
+struct SplitPos {
+  int ny, hx;
+  __device__ __forceinline__ int operator()(int, int i, int j, int k) const {
+    return 2 * hx * (j + ny * k) + (i & 1) * hx + (i >> 1);
+  }
+};
+
 // A x at one cell, in the reference's accumulation order.
-template <class T, class Ld = PlainLoad>
+template <class T, class Ld = PlainLoad, class Pos = NaturalPos>
 __device__ __forceinline__ T row_value(const Level<T>& L, const T* x, int i,
-                                       int j, int k, int c) {
+                                       int j, int k, int c, Pos pos = Pos()) {
   const int plane = L.nx * L.ny;
-  const T xc = Ld::get(x + c);
-  const T xm = i > 0 ? Ld::get(x + c - 1) : ((L.neumann & 1u) ? xc : T(0));
-  const T xp = i + 1 < L.nx ? Ld::get(x + c + 1) : ((L.neumann & 2u) ? xc : T(0));
-  const T ym = j > 0 ? Ld::get(x + c - L.nx) : ((L.neumann & 4u) ? xc : T(0));
-  const T yp = j + 1 < L.ny ? Ld::get(x + c + L.nx) : ((L.neumann & 8u) ? xc : T(0));
-  const T zm = k > 0 ? Ld::get(x + c - plane) : ((L.neumann & 16u) ? xc : T(0));
-  const T zp = k + 1 < L.nz ? Ld::get(x + c + plane) : ((L.neumann & 32u) ? xc : T(0));
+  const T xc = Ld::get(x + pos(c, i, j, k));
+  const T xm = i > 0 ? Ld::get(x + pos(c - 1, i - 1, j, k))
+                     : ((L.neumann & 1u) ? xc : T(0));
+  const T xp = i + 1 < L.nx ? Ld::get(x + pos(c + 1, i + 1, j, k))
+                            : ((L.neumann & 2u) ? xc : T(0));
+  const T ym = j > 0 ? Ld::get(x + pos(c - L.nx, i, j - 1, k))
+                     : ((L.neumann & 4u) ? xc : T(0));
+  const T yp = j + 1 < L.ny ? Ld::get(x + pos(c + L.nx, i, j + 1, k))
+                            : ((L.neumann & 8u) ? xc : T(0));
+  const T zm = k > 0 ? Ld::get(x + pos(c - plane, i, j, k - 1))
+                     : ((L.neumann & 16u) ? xc : T(0));
+  const T zp = k + 1 < L.nz ? Ld::get(x + pos(c + plane, i, j, k + 1))
+                            : ((L.neumann & 32u) ? xc : T(0));
   const int fxi = face_x_index(L, c, j, k);
   const int fyi = face_y_index(L, c, k);
   T v = L.diag[c] * xc;

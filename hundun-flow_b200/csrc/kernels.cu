@@ -96,6 +96,14 @@ __device__ void apply_scalar_op(Scalars* sc, int op, double sum) {
   }
 }
 
+// Index of natural cell c in a vector of layout v.
+__device__ __forceinline__ int vec_pos(const VecLayout& v, int c) {
+  if (v.hx == 0) return c;
+  const int row = c / v.nx;
+  const int i = c - row * v.nx;
+  return 2 * v.hx * row + (i & 1) * v.hx + (i >> 1);
+}
+
 // ---------------------------------------------------------------------------
 // Level operators: apply_level_matrix / apply_level_defect
 // (src/solver_mg.cpp:2569-2767).
@@ -114,14 +122,18 @@ __global__ void k_level_apply(Level<T> L, const T* __restrict__ x,
 
 template <class T>
 __global__ void k_level_defect(Level<T> L, const T* __restrict__ x,
-                               const T* __restrict__ b, T* __restrict__ r) {
+                               const T* __restrict__ b, T* __restrict__ r, int hx) {
   grid_dependency_sync();
   const int n = L.nx * L.ny * L.nz;
+  const SplitPos sp{L.ny, hx};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
     int i, j, k;
     cell_coords(c, L.nx, L.ny, i, j, k);
-    r[c] = b[c] - row_value(L, x, i, j, k, c);
+    if (hx == 0)
+      r[c] = b[c] - row_value(L, x, i, j, k, c);
+    else
+      r[c] = b[sp(c, i, j, k)] - row_value<T, PlainLoad, SplitPos>(L, x, i, j, k, c, sp);
   }
 }
 
@@ -227,12 +239,14 @@ template <class T>
 __global__ void k_defect_restrict(Level<T> F, const T* __restrict__ x,
                                   const T* __restrict__ b, Level<T> C,
                                   T* __restrict__ cb, T* __restrict__ cx,
-                                  int mask) {
+                                  int mask, int hx) {
   grid_dependency_sync();
   const int n = C.nx * C.ny * C.nz;
+  const SplitPos sp{F.ny, hx};
   for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
        cc += gridDim.x * blockDim.x) {
-    cb[cc] = defect_restrict_cell<T>(F, x, b, C, mask, cc);
+    cb[cc] = hx == 0 ? defect_restrict_cell<T>(F, x, b, C, mask, cc)
+                     : defect_restrict_cell<T, PlainLoad, SplitPos>(F, x, b, C, mask, cc, sp);
     cx[cc] = T(0);
   }
 }
@@ -262,16 +276,31 @@ __global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
 }
 
 // Trilinear prolongation and add, zero on solid cells (prolongate_cell):
-// one fine cell per thread, the coarse correction through the read-only
-// path.
+// one fine vector entry per thread (natural order, or split rows walked
+// entry by entry so that stores stay contiguous), the coarse correction
+// through the read-only path.
 template <class T>
 __global__ void k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C,
-                             const T* __restrict__ cx, int mask) {
+                             const T* __restrict__ cx, int mask, int hx) {
   grid_dependency_sync();
-  const int n = F.nx * F.ny * F.nz;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  x[c] = prolongate_cell<T, PlainLoad, RoLoad>(F, x, C, cx, mask, c);
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k, c;
+  if (hx == 0) {
+    c = p;
+    if (c >= F.nx * F.ny * F.nz) return;
+    cell_coords(c, F.nx, F.ny, i, j, k);
+  } else {
+    const int row = p / (2 * hx);
+    if (row >= F.ny * F.nz) return;
+    const int w = p - row * 2 * hx;
+    const int odd = w >= hx ? 1 : 0;
+    i = 2 * (w - odd * hx) + odd;
+    if (i >= F.nx) return;  // the odd half's padding slot
+    k = row / F.ny;
+    j = row - k * F.ny;
+    c = i + F.nx * row;
+  }
+  x[p] = prolongate_cell<T, PlainLoad, RoLoad>(F, x, C, cx, mask, c, i, j, k, p);
 }
 
 // Coarsest level: `sweeps` smoother sweeps in one CTA (mg_cycle coarse
@@ -325,13 +354,14 @@ __global__ void k_coarse_solve(Level<TC> L, T* x, const T* b, TC* xs, TC* bs,
 template <class T>
 __global__ void k_mg_enter(int n, const double* __restrict__ r,
                            const uint8_t* __restrict__ active,
-                           T* __restrict__ b, T* __restrict__ x) {
+                           T* __restrict__ b, T* __restrict__ x, VecLayout v, bool zero_x) {
   grid_dependency_sync();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
     const bool on = active == nullptr || active[c] != 0;
-    b[c] = on ? static_cast<T>(r[c]) : T(0);
-    x[c] = T(0);
+    const int at = vec_pos(v, c);
+    b[at] = on ? static_cast<T>(r[c]) : T(0);
+    if (zero_x) x[at] = T(0);
   }
 }
 
@@ -339,24 +369,26 @@ template <class T>
 __global__ void k_mg_exit(int n, const T* __restrict__ x,
                           const uint8_t* __restrict__ active,
                           const double* __restrict__ scale_ptr,
-                          double* __restrict__ z) {
+                          double* __restrict__ z, VecLayout v) {
   grid_dependency_sync();
   const double scale = scale_ptr == nullptr ? 1.0 : *scale_ptr;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
     const bool on = active == nullptr || active[c] != 0;
-    z[c] = on ? static_cast<double>(x[c]) * scale : 0.0;
+    z[c] = on ? static_cast<double>(x[vec_pos(v, c)]) * scale : 0.0;
   }
 }
 
 template <class T>
 __global__ void k_diagonal_solve(int n, const T* __restrict__ b,
                                  const T* __restrict__ diag,
-                                 T* __restrict__ x) {
+                                 T* __restrict__ x, VecLayout v) {
   grid_dependency_sync();
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x)
-    x[c] = b[c] / diag[c];
+       c += gridDim.x * blockDim.x) {
+    const int at = vec_pos(v, c);
+    x[at] = b[at] / diag[c];
+  }
 }
 
 template <class T>
@@ -1195,8 +1227,8 @@ void launch_level_apply(cudaStream_t s, const Level<T>& L, const T* x, T* y) {
 }
 template <class T>
 void launch_level_defect(cudaStream_t s, const Level<T>& L, const T* x,
-                         const T* b, T* r) {
-  launch(k_level_defect<T>, grid_for(HFPS_CELLS(L)), kThreads, 0, s, L, x, b, r);
+                         const T* b, T* r, int hx) {
+  launch(k_level_defect<T>, grid_for(HFPS_CELLS(L)), kThreads, 0, s, L, x, b, r, hx);
 }
 template <class T>
 void launch_rb_color(cudaStream_t s, const Level<T>& L, T* x, const T* b,
@@ -1214,9 +1246,9 @@ void launch_chebyshev_stage(cudaStream_t s, const Level<T>& L, const T* x,
 template <class T>
 void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
                             const T* b, const Level<T>& C, T* cb, T* cx,
-                            int mask) {
+                            int mask, int hx) {
   launch(k_defect_restrict<T>, grid_for(HFPS_CELLS(C)), kThreads, 0, s, F, x, b, C, cb,
-                                                                   cx, mask);
+                                                                   cx, mask, hx);
 }
 template <class T>
 void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
@@ -1225,10 +1257,11 @@ void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
 }
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
-                       const Level<T>& C, const T* cx, int mask) {
-  const long long cells = HFPS_CELLS(F);
-  launch(k_prolongate<T>, static_cast<int>((cells + kThreads - 1) / kThreads), kThreads, 0, s, 
-      F, x, C, cx, mask);
+                       const Level<T>& C, const T* cx, int mask, int hx) {
+  const long long entries =
+      hx == 0 ? HFPS_CELLS(F) : 2LL * hx * F.ny * static_cast<long long>(F.nz);
+  launch(k_prolongate<T>, static_cast<int>((entries + kThreads - 1) / kThreads), kThreads, 0, s,
+         F, x, C, cx, mask, hx);
 }
 template <class T, class TC>
 void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
@@ -1239,18 +1272,18 @@ void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
 }
 template <class T>
 void launch_mg_enter(cudaStream_t s, int n, const double* r,
-                     const uint8_t* active, T* b, T* x) {
-  launch(k_mg_enter<T>, grid_for(n), kThreads, 0, s, n, r, active, b, x);
+                     const uint8_t* active, T* b, T* x, VecLayout v, bool zero_x) {
+  launch(k_mg_enter<T>, grid_for(n), kThreads, 0, s, n, r, active, b, x, v, zero_x);
 }
 template <class T>
 void launch_mg_exit(cudaStream_t s, int n, const T* x, const uint8_t* active,
-                    const double* scale_ptr, double* z) {
-  launch(k_mg_exit<T>, grid_for(n), kThreads, 0, s, n, x, active, scale_ptr, z);
+                    const double* scale_ptr, double* z, VecLayout v) {
+  launch(k_mg_exit<T>, grid_for(n), kThreads, 0, s, n, x, active, scale_ptr, z, v);
 }
 template <class T>
 void launch_diagonal_solve(cudaStream_t s, int n, const T* b, const T* diag,
-                           T* x) {
-  launch(k_diagonal_solve<T>, grid_for(n), kThreads, 0, s, n, b, diag, x);
+                           T* x, VecLayout v) {
+  launch(k_diagonal_solve<T>, grid_for(n), kThreads, 0, s, n, b, diag, x, v);
 }
 template <class T>
 void launch_mg_projection(cudaStream_t s, int n, const double* r,
@@ -1439,23 +1472,24 @@ void launch_adjoint_source(cudaStream_t s, int n, const double* dl_dp,
 #define HFPS_INSTANTIATE(T)                                                        \
   template void launch_level_apply<T>(cudaStream_t, const Level<T>&, const T*, T*); \
   template void launch_level_defect<T>(cudaStream_t, const Level<T>&, const T*,    \
-                                       const T*, T*);                              \
+                                       const T*, T*, int);                         \
   template void launch_rb_color<T>(cudaStream_t, const Level<T>&, T*, const T*,    \
                                    int);                                           \
   template void launch_chebyshev_stage<T>(cudaStream_t, const Level<T>&, const T*, \
                                           const T*, T*, T*, T, T, int);            \
   template void launch_defect_restrict<T>(cudaStream_t, const Level<T>&, const T*, \
-                                          const T*, const Level<T>&, T*, T*, int); \
+                                          const T*, const Level<T>&, T*, T*, int,  \
+                                          int);                                    \
   template void launch_restrict<T>(cudaStream_t, const Level<T>&, const T*,        \
                                    const Level<T>&, T*, T*, int);                  \
   template void launch_prolongate<T>(cudaStream_t, const Level<T>&, T*,            \
-                                     const Level<T>&, const T*, int);              \
+                                     const Level<T>&, const T*, int, int);         \
   template void launch_mg_enter<T>(cudaStream_t, int, const double*,               \
-                                   const uint8_t*, T*, T*);                        \
+                                   const uint8_t*, T*, T*, VecLayout, bool);       \
   template void launch_mg_exit<T>(cudaStream_t, int, const T*, const uint8_t*,     \
-                                  const double*, double*);                         \
+                                  const double*, double*, VecLayout);              \
   template void launch_diagonal_solve<T>(cudaStream_t, int, const T*, const T*,    \
-                                         T*);                                      \
+                                         T*, VecLayout);                           \
   template void launch_mg_projection<T>(cudaStream_t, int, const double*,          \
                                         const uint8_t*, const T*, Reduce);
 

@@ -53,12 +53,21 @@ struct Reduce {
 
 int reduction_blocks(long long items);
 
+// Layout of a level's vectors (x, b): hx == 0 the natural x-fastest order,
+// otherwise split rows (SplitPos) whose even- and odd-i halves are hx cells
+// long, 2 * hx * ny * nz values in all.  Coefficients and every other vector
+// stay in the natural order.
+struct VecLayout {
+  int nx, ny, hx;
+};
+
 // ---- level operators (T = double or float) -------------------------------
 template <class T>
 void launch_level_apply(cudaStream_t s, const Level<T>& L, const T* x, T* y);
+// r (natural order) = b - A x with x, b in layout hx.
 template <class T>
 void launch_level_defect(cudaStream_t s, const Level<T>& L, const T* x,
-                         const T* b, T* r);
+                         const T* b, T* r, int hx = 0);
 template <class T>
 void launch_rb_color(cudaStream_t s, const Level<T>& L, T* x, const T* b,
                      int color);
@@ -66,16 +75,17 @@ template <class T>
 void launch_chebyshev_stage(cudaStream_t s, const Level<T>& L, const T* x,
                             const T* b, T* direction, T* next,
                             T previous_factor, T residual_factor, int first);
+// Fine x, b in layout hx; coarse vectors natural.
 template <class T>
 void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
                             const T* b, const Level<T>& C, T* cb, T* cx,
-                            int coarsen_mask);
+                            int coarsen_mask, int hx = 0);
 template <class T>
 void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
                      const Level<T>& C, T* cb, T* cx, int coarsen_mask);
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
-                       const Level<T>& C, const T* cx, int coarsen_mask);
+                       const Level<T>& C, const T* cx, int coarsen_mask, int hx = 0);
 // ---- zebra line relaxation (kernels_line.cu) --------------------------------
 // Line-colour passes with more lines than this run the chunked-scan solve
 // (lanes across lines, warps along chunks of one line); fewer lines run PCR
@@ -90,10 +100,14 @@ int line_kind(int nx, int ny, int nz, int axis);
 size_t line_factor_values(int nx, int ny, int nz, int axis);
 template <class T>
 void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac);
-// One zebra colour of line relaxation along `axis`.
+// One zebra colour of line relaxation along `axis`, x and b in layout hx
+// (split rows only with the scan solve, axis 1 or 2).  zero_other: the other
+// colour's x is known to be zero (not read); zero_self: this colour's x is
+// (the first pass and the first sweep of a cycle started from x = 0).
 template <class T>
 void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
-                      const T* fac, T* scratch, int axis, int color);
+                      const T* fac, T* scratch, int axis, int color, int hx = 0,
+                      bool zero_other = false, bool zero_self = false);
 // Coarsest level in line mode with x/rhs resident in shared memory; returns
 // false when the level is too large for that form.  With `columns`, launches
 // 2n blocks that write the columns of the sweeps' affine map x_out = P x_in
@@ -117,17 +131,18 @@ void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
                          int line_axis);
 
 // ---- MG entry/exit ------------------------------------------------------
-// b = active ? r : 0 (converted to T), x = 0.
+// b = active ? r : 0 (converted to T), and x = 0 when zero_x; b and x in
+// layout v, r natural.
 template <class T>
 void launch_mg_enter(cudaStream_t s, int n, const double* r,
-                     const uint8_t* active, T* b, T* x);
+                     const uint8_t* active, T* b, T* x, VecLayout v, bool zero_x);
 // z = active ? x * scale : 0 (scale read from device when scale_ptr).
 template <class T>
 void launch_mg_exit(cudaStream_t s, int n, const T* x, const uint8_t* active,
-                    const double* scale_ptr, double* z);
+                    const double* scale_ptr, double* z, VecLayout v);
 template <class T>
 void launch_diagonal_solve(cudaStream_t s, int n, const T* b, const T* diag,
-                           T* x);
+                           T* x, VecLayout v);
 // Projection sums for the residual-minimising MG scale (level-0, FP64 r).
 template <class T>
 void launch_mg_projection(cudaStream_t s, int n, const double* r,

@@ -34,8 +34,15 @@ namespace {
 // unconditional, so a thread can keep many rows' loads in flight.  The
 // arithmetic and its order are line_rhs's.  Transverse neighbours belong to
 // the other colour, which a colour pass never writes, so they are read
-// through the read-only path.
-template <class T, int AXIS>
+// through the read-only path.  With hx > 0 the vectors are in split rows
+// (SplitPos): an x neighbour sits in the other half of the row, a y or z
+// neighbour in the same half of the previous or next row.  A neighbour
+// outside the level reads the cell itself (Neumann), so it counts as this
+// colour's value for the zero flags of the first sweep.
+// Variants of a scan colour pass by what is known of x (LineRhs::row).
+enum ScanMode : int { kScanNormal = 0, kScanOwnZero = 1, kScanFresh = 2 };
+
+template <class T, int AXIS, bool SPLIT>
 struct LineRhs {
   static constexpr int kA0 = AXIS == 0 ? 1 : 0;  // first transverse axis
   static constexpr int kA1 = AXIS == 2 ? 1 : 2;  // second transverse axis
@@ -43,6 +50,7 @@ struct LineRhs {
   int fbase[2], fstride[2], fhigh[2];
   int off[4];
   bool keep[4];
+  bool self[4];   // the neighbour is the cell itself (outside the level)
   T end_low, end_high;   // line-end boundary faces (rows 0 and extent-1)
   bool lkeep_low, lkeep_high;
 
@@ -71,7 +79,7 @@ struct LineRhs {
     (void)nz;
   }
 
-  __device__ LineRhs(const Level<T>& L, int fa, int fb) {
+  __device__ LineRhs(const Level<T>& L, int fa, int fb, int hx) {
     int i0, j0, k0;
     line_cell(AXIS, fa, fb, 0, i0, j0, k0);
     const int idx[3] = {i0, j0, k0};
@@ -83,8 +91,16 @@ struct LineRhs {
       const int a = axes[n];
       axis_faces(L, a, i0, j0, k0, AXIS, face[n], fbase[n], fstride[n], fhigh[n]);
       const bool low_in = idx[a] > 0, high_in = idx[a] + 1 < ext[a];
-      off[2 * n] = low_in ? -step[a] : 0;
-      off[2 * n + 1] = high_in ? step[a] : 0;
+      int lo = -step[a], hi = step[a];
+      if (SPLIT) {
+        const int odd = i0 & 1;
+        lo = a == 0 ? (odd ? -hx : hx - 1) : (a == 1 ? -2 * hx : -2 * hx * L.ny);
+        hi = a == 0 ? (odd ? 1 - hx : hx) : (a == 1 ? 2 * hx : 2 * hx * L.ny);
+      }
+      off[2 * n] = low_in ? lo : 0;
+      off[2 * n + 1] = high_in ? hi : 0;
+      self[2 * n] = !low_in;
+      self[2 * n + 1] = !high_in;
       keep[2 * n] = low_in || ((L.neumann >> (2 * a)) & 1u);
       keep[2 * n + 1] = high_in || ((L.neumann >> (2 * a + 1)) & 1u);
     }
@@ -97,21 +113,33 @@ struct LineRhs {
     lkeep_high = (L.neumann >> (2 * AXIS + 1)) & 1u;
   }
 
+  // Row s, c its vector index.  MODE kScanFresh: x is zero everywhere and
+  // not read.  kScanOwnZero: this colour's x is zero; its values (the cell
+  // itself, read where a neighbour lies outside the level) are still loaded,
+  // so that every load stays unconditional, and then replaced by zero.
+  template <int MODE>
   __device__ __forceinline__ T row(const T* x, const T* __restrict__ rhs, int c,
                                    int s, int extent) const {
     T d = __ldg(rhs + c);
 #pragma unroll
     for (int n = 0; n < 2; ++n) {
       const int f = fbase[n] + s * fstride[n];
-      const T lo = __ldg(x + c + off[2 * n]);
-      const T hi = __ldg(x + c + off[2 * n + 1]);
+      T lo = T(0), hi = T(0);
+      if (MODE != kScanFresh) {
+        lo = __ldg(x + c + off[2 * n]);
+        hi = __ldg(x + c + off[2 * n + 1]);
+      }
+      if (MODE == kScanOwnZero) {
+        lo = self[2 * n] ? T(0) : lo;
+        hi = self[2 * n + 1] ? T(0) : hi;
+      }
       d += __ldg(face[n] + f) * (keep[2 * n] ? lo : T(0));
       d += __ldg(face[n] + f + fhigh[n]) * (keep[2 * n + 1] ? hi : T(0));
     }
-    const T self = x[c];
-    const T dl = d + end_low * (lkeep_low ? self : T(0));
+    const T self_value = MODE == kScanNormal ? x[c] : T(0);
+    const T dl = d + end_low * (lkeep_low ? self_value : T(0));
     d = s == 0 ? dl : d;
-    const T dh = d + end_high * (lkeep_high ? self : T(0));
+    const T dh = d + end_high * (lkeep_high ? self_value : T(0));
     return s + 1 == extent ? dh : d;
   }
 };
@@ -226,10 +254,10 @@ __global__ void k_scan_factors(Level<T> L, int axis, T* __restrict__ fac) {
 // One zebra colour: blockDim = (LPB lines, S chunks), chunk q holds rows
 // [q*m, min(extent, (q+1)*m) - 1] with m <= ScanConfig<T>::rows.  Shared memory holds
 // the chunk compositions: forward (A, B) and backward (A, B), S x LPB each.
-template <class T, int AXIS, int LPB>
+template <class T, int AXIS, int LPB, int MODE, bool SPLIT>
 __global__ void __launch_bounds__(ScanConfig<T>::threads)
     k_line_scan_color(Level<T> L, T* x, const T* __restrict__ rhs,
-                      const T* __restrict__ fac, int color, int m) {
+                      const T* __restrict__ fac, int color, int m, int hx) {
   grid_dependency_sync();
   extern __shared__ unsigned char scan_smem[];
   const int S = blockDim.y;
@@ -248,8 +276,17 @@ __global__ void __launch_bounds__(ScanConfig<T>::threads)
   const int fb = t / ha;
   const int fa = 2 * (t - fb * ha) + ((fb + color) & 1);
   const bool valid = t < ha * b_extent && fa < a_extent;
+  // Vector index of row 0 and its step per row (natural or split rows).
   int base = 0, stride = 0;
-  if (valid) line_geometry(L, AXIS, fa, fb, base, stride);
+  if (valid) {
+    line_geometry(L, AXIS, fa, fb, base, stride);
+    if (SPLIT) {
+      int i0, j0, k0;
+      line_cell(AXIS, fa, fb, 0, i0, j0, k0);
+      base = 2 * hx * (j0 + L.ny * k0) + (i0 & 1) * hx + (i0 >> 1);
+      stride = AXIS == 1 ? 2 * hx : 2 * hx * L.ny;
+    }
+  }
   const int r0 = q * m;
   const int rows = valid ? max(0, min(m, extent - r0)) : 0;
   const int row = lay.colour_lines;
@@ -263,12 +300,13 @@ __global__ void __launch_bounds__(ScanConfig<T>::threads)
   const auto srow = [&](int u) { return min(r0 + u, extent - 1); };
 
   // Pass 1: right-hand sides scaled by 1/den, and the forward composition.
-  const LineRhs<T, AXIS> lr(L, valid ? fa : 0, valid ? fb : 0);
+  const LineRhs<T, AXIS, SPLIT> lr(L, valid ? fa : 0, valid ? fb : 0, hx);
   constexpr int kScanRows = ScanConfig<T>::rows;
   T v[kScanRows];
 #pragma unroll
   for (int u = 0; u < kScanRows; ++u)
-    v[u] = lr.row(x, rhs, base + srow(u) * stride, srow(u), extent) * __ldg(inv + srow(u) * row);
+    v[u] = lr.template row<MODE>(x, rhs, base + srow(u) * stride, srow(u), extent) *
+           __ldg(inv + srow(u) * row);
   T A = T(1), B = T(0);
 #pragma unroll
   for (int u = 0; u < kScanRows; ++u) {
@@ -524,25 +562,51 @@ ScanShape scan_shape(long long per_color, int extent) {
   return sh;
 }
 
+struct ScanFlags {
+  int hx;
+  bool zero_other, zero_self;
+};
+
 template <class T, int AXIS, int LPB>
 void launch_scan(cudaStream_t s, const Level<T>& L, T* x, const T* b, const T* fac,
-                 int color, long long per_color, const ScanShape& sh) {
+                 int color, long long per_color, const ScanShape& sh, ScanFlags f) {
   const int blocks = static_cast<int>((per_color + LPB - 1) / LPB);
   const size_t smem = static_cast<size_t>(4) * sh.chunks * LPB * sizeof(T);
-  launch(k_line_scan_color<T, AXIS, LPB>, blocks, dim3(LPB, sh.chunks), smem, s, L, x, b, fac, color,
-                                                                             sh.rows);
+  // The zero variants and split rows only on y- and z-line levels (x-line
+  // levels keep the natural order and always read x, which the cycle has
+  // cleared).
+  const dim3 block(LPB, sh.chunks);
+  constexpr bool kYZ = AXIS != 0;
+  const int mode = !kYZ ? kScanNormal
+                        : (f.zero_other && f.zero_self ? kScanFresh
+                                                       : (f.zero_self ? kScanOwnZero : kScanNormal));
+  const bool split = kYZ && f.hx != 0;
+#define HFPS_SCAN_LAUNCH(MODE, SPLIT)                                                         \
+  launch(k_line_scan_color<T, AXIS, LPB, kYZ ? MODE : kScanNormal, kYZ && SPLIT>, blocks, block, \
+         smem, s, L, x, b, fac, color, sh.rows, f.hx)
+  if (mode == kScanFresh) {
+    if (split) HFPS_SCAN_LAUNCH(kScanFresh, true);
+    else HFPS_SCAN_LAUNCH(kScanFresh, false);
+  } else if (mode == kScanOwnZero) {
+    if (split) HFPS_SCAN_LAUNCH(kScanOwnZero, true);
+    else HFPS_SCAN_LAUNCH(kScanOwnZero, false);
+  } else {
+    if (split) HFPS_SCAN_LAUNCH(kScanNormal, true);
+    else HFPS_SCAN_LAUNCH(kScanNormal, false);
+  }
+#undef HFPS_SCAN_LAUNCH
 }
 
 template <class T, int AXIS>
 void launch_scan_axis(cudaStream_t s, const Level<T>& L, T* x, const T* b, const T* fac,
-                      int color, long long per_color, const ScanShape& sh) {
+                      int color, long long per_color, const ScanShape& sh, ScanFlags f) {
   switch (sh.lpb) {
-    case 32: launch_scan<T, AXIS, 32>(s, L, x, b, fac, color, per_color, sh); break;
-    case 16: launch_scan<T, AXIS, 16>(s, L, x, b, fac, color, per_color, sh); break;
-    case 8: launch_scan<T, AXIS, 8>(s, L, x, b, fac, color, per_color, sh); break;
-    case 4: launch_scan<T, AXIS, 4>(s, L, x, b, fac, color, per_color, sh); break;
-    case 2: launch_scan<T, AXIS, 2>(s, L, x, b, fac, color, per_color, sh); break;
-    default: launch_scan<T, AXIS, 1>(s, L, x, b, fac, color, per_color, sh); break;
+    case 32: launch_scan<T, AXIS, 32>(s, L, x, b, fac, color, per_color, sh, f); break;
+    case 16: launch_scan<T, AXIS, 16>(s, L, x, b, fac, color, per_color, sh, f); break;
+    case 8: launch_scan<T, AXIS, 8>(s, L, x, b, fac, color, per_color, sh, f); break;
+    case 4: launch_scan<T, AXIS, 4>(s, L, x, b, fac, color, per_color, sh, f); break;
+    case 2: launch_scan<T, AXIS, 2>(s, L, x, b, fac, color, per_color, sh, f); break;
+    default: launch_scan<T, AXIS, 1>(s, L, x, b, fac, color, per_color, sh, f); break;
   }
 }
 
@@ -590,7 +654,8 @@ void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac) {
 
 template <class T>
 void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
-                      const T* fac, T* scratch, int axis, int color) {
+                      const T* fac, T* scratch, int axis, int color, int hx,
+                      bool zero_other, bool zero_self) {
   (void)scratch;
   const int extent = line_extent(axis, L.nx, L.ny, L.nz);
   const int a_extent = axis == 0 ? L.ny : L.nx;
@@ -600,9 +665,10 @@ void launch_line_pass(cudaStream_t s, const Level<T>& L, T* x, const T* b,
   if (kind == kLineNone) return;
   if (kind == kLineScan) {
     const ScanShape sh = scan_shape<T>(per_color, extent);
-    if (axis == 0) launch_scan_axis<T, 0>(s, L, x, b, fac, color, per_color, sh);
-    else if (axis == 1) launch_scan_axis<T, 1>(s, L, x, b, fac, color, per_color, sh);
-    else launch_scan_axis<T, 2>(s, L, x, b, fac, color, per_color, sh);
+    const ScanFlags f{axis == 0 ? 0 : hx, zero_other, zero_self};
+    if (axis == 0) launch_scan_axis<T, 0>(s, L, x, b, fac, color, per_color, sh, f);
+    else if (axis == 1) launch_scan_axis<T, 1>(s, L, x, b, fac, color, per_color, sh, f);
+    else launch_scan_axis<T, 2>(s, L, x, b, fac, color, per_color, sh, f);
     return;
   }
   int P, lpb, steps;
@@ -661,9 +727,10 @@ bool launch_coarse_line(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
 template void launch_line_factors<double>(cudaStream_t, const Level<double>&, int, double*);
 template void launch_line_factors<float>(cudaStream_t, const Level<float>&, int, float*);
 template void launch_line_pass<double>(cudaStream_t, const Level<double>&, double*,
-                                       const double*, const double*, double*, int, int);
+                                       const double*, const double*, double*, int, int, int,
+                                       bool, bool);
 template void launch_line_pass<float>(cudaStream_t, const Level<float>&, float*, const float*,
-                                      const float*, float*, int, int);
+                                      const float*, float*, int, int, int, bool, bool);
 template bool launch_coarse_line<double, double>(cudaStream_t, const Level<double>&, double*,
                                                  const double*, const double*, int, int, bool);
 template bool launch_coarse_line<float, double>(cudaStream_t, const Level<double>&, float*,

@@ -211,9 +211,10 @@ __device__ __forceinline__ void chebyshev_cell(const Level<T>& L, const T* x, co
 // Retained defect + restriction at coarse cell cc (apply_level_defect
 // followed by restrict_residual, src/solver_mg.cpp:3633-3721): the defects
 // of the children summed in dz, dy, dx order.
-template <class T, class Ld = PlainLoad>
+template <class T, class Ld = PlainLoad, class Pos = NaturalPos>
 __device__ __forceinline__ T defect_restrict_cell(const Level<T>& F, const T* x, const T* b,
-                                                  const Level<T>& C, int mask, int cc) {
+                                                  const Level<T>& C, int mask, int cc,
+                                                  Pos pos = Pos()) {
   const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
   int ci, cj, ck;
   cell_coords(cc, C.nx, C.ny, ci, cj, ck);
@@ -225,7 +226,7 @@ __device__ __forceinline__ T defect_restrict_cell(const Level<T>& F, const T* x,
         const int fi = xb + dx, fj = yb + dy, fk = zb + dz;
         if (fi >= F.nx || fj >= F.ny || fk >= F.nz) continue;
         const int fc = fi + F.nx * (fj + F.ny * fk);
-        sum += Ld::get(b + fc) - row_value<T, Ld>(F, x, fi, fj, fk, fc);
+        sum += Ld::get(b + pos(fc, fi, fj, fk)) - row_value<T, Ld>(F, x, fi, fj, fk, fc, pos);
       }
   return sum;
 }
@@ -264,15 +265,14 @@ __device__ __forceinline__ void interp_axis(int fine, int coarsened,
 // unconditionally (a degenerate axis repeats its one index) and the terms
 // are added in the reference's order (z outer, x inner) with the absent
 // ones skipped by selects, so all loads of a cell are in flight together.
-// LdC reads the coarse correction.
+// LdC reads the coarse correction; the cell's x sits at x[at].
 template <class T, class Ld = PlainLoad, class LdC = PlainLoad>
 __device__ __forceinline__ T prolongate_cell(const Level<T>& F, const T* x, const Level<T>& C,
-                                             const T* cx, int mask, int c) {
+                                             const T* cx, int mask, int c, int i, int j, int k,
+                                             int at) {
   const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
   const bool fluid = F.fluid[c] != 0;
-  const T old = Ld::get(x + c);
-  int i, j, k;
-  cell_coords(c, F.nx, F.ny, i, j, k);
+  const T old = Ld::get(x + at);
   int xi[2], yi[2], zi[2];
   double xw, yw, zw;
   interp_axis(i, mx, C.nx, xi[0], xi[1], xw);

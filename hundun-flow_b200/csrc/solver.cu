@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <limits>
 #include <type_traits>
 
@@ -218,6 +219,19 @@ Status Solver::allocate() {
       if ((s.line_mask & (1 << a)) && line_kind(s.n[0], s.n[1], s.n[2], a) == kLineNone)
         return fail(HFPS_INVALID_PLAN, kDetailPlan, "line relaxation: line longer than 2048 cells");
   const int levels = static_cast<int>(shapes.size());
+  // Split rows for the finest level's MG x and b when it relaxes y- or
+  // z-lines with the chunked scan: a colour pass then reads and writes whole
+  // halves of rows instead of every other cell (HFPS_SPLIT0=0 keeps the
+  // natural order).
+  int split0 = 0;
+  {
+    const Shape& s0 = shapes[0];
+    const char* env = std::getenv("HFPS_SPLIT0");
+    const int axis = s0.line_mask == 2 ? 1 : (s0.line_mask == 4 ? 2 : -1);
+    const bool scan = axis > 0 && line_kind(s0.n[0], s0.n[1], s0.n[2], axis) == kLineScan;
+    if (scan && !(env != nullptr && env[0] == '0')) split0 = (s0.n[0] + 1) / 2;
+    first_sweep_zero_ = scan && policy_.pre_sweeps >= 1;
+  }
   // Sizes.
   size_t bytes = 0;
   const auto add = [&](size_t b) {
@@ -240,11 +254,15 @@ Status Solver::allocate() {
     const size_t fz = static_cast<size_t>(s.n[0]) * s.n[1] * (s.n[2] + 1);
     max_faces = std::max({max_faces, fx, fy, fz});
     Offsets& o = off[l];
+    // x and b hold 2 * hx * ny * nz values in split rows.
+    const size_t cv = l == 0 && split0 > 0
+                          ? 2 * static_cast<size_t>(split0) * s.n[1] * s.n[2]
+                          : c;
     o.d = add(c * 8); o.fx = add(fx * 8); o.fy = add(fy * 8); o.fz = add(fz * 8);
-    o.x = add(c * 8); o.b = add(c * 8); o.r = add(c * 8); o.t = add(c * 8);
+    o.x = add(cv * 8); o.b = add(cv * 8); o.r = add(c * 8); o.t = add(c * 8);
     o.vol = add(c * 8); o.fluid = add(c);
     o.d32 = add(c * 4); o.fx32 = add(fx * 4); o.fy32 = add(fy * 4); o.fz32 = add(fz * 4);
-    o.x32 = add(c * 4); o.b32 = add(c * 4); o.r32 = add(c * 4); o.t32 = add(c * 4);
+    o.x32 = add(cv * 4); o.b32 = add(cv * 4); o.r32 = add(c * 4); o.t32 = add(c * 4);
     for (int a = 0; a < 3; ++a) {
       o.lf64[a] = o.lf32[a] = SIZE_MAX;
       if (!(s.line_mask & (1 << a))) continue;
@@ -344,6 +362,7 @@ Status Solver::allocate() {
     a.nz = b.nz = s.n[2];
     a.coarsen_mask = b.coarsen_mask = s.coarsen_mask;
     a.line_mask = b.line_mask = s.line_mask;
+    a.split = b.split = l == 0 ? split0 : 0;
     // build_levels: Chebyshev only on non-coarsest point levels
     // (src/solver_mg.cpp:1060-1073).
     a.chebyshev = b.chebyshev =
@@ -676,9 +695,11 @@ Status Solver::correct_flux(const double* correction, const double* cx, const do
 // ---------------------------------------------------------------------------
 // MG cycle (mg_cycle, src/solver_mg.cpp:4192-4338).
 
+// x_zero: the level's x is zero on entry (a cycle's first visit), which the
+// chunked scan uses to skip reading it in the first sweep.
 template <class T>
 void Solver::smooth(std::vector<DeviceLevel<T>>& levels, int level, int sweeps,
-                    bool reverse) {
+                    bool reverse, bool x_zero) {
   DeviceLevel<T>& L = levels[level];
   const Level<T> view = L.view(neumann_);
   if (L.line_mask == 0) {
@@ -711,12 +732,17 @@ void Solver::smooth(std::vector<DeviceLevel<T>>& levels, int level, int sweeps,
   }
   // smooth(): line relaxation along every strong axis, reversed on the way
   // up (src/solver_mg.cpp:3566-3589); zebra colour order per sweep.
+  // In the first sweep from x = 0 (one line axis), the first pass reads no
+  // x and the second reads only the colour the first wrote.
+  const bool one_axis = (L.line_mask & (L.line_mask - 1)) == 0;
   const auto run_axis = [&](int axis) {
     const int first = reverse ? 1 : 0;
     for (int s = 0; s < sweeps; ++s)
-      for (int pass = 0; pass < 2; ++pass)
+      for (int pass = 0; pass < 2; ++pass) {
+        const bool fresh = x_zero && one_axis && s == 0;
         launch_line_pass<T>(stream_, view, L.x, L.b, L.lfac[axis], L.r, axis,
-                            (first + pass) & 1);
+                            (first + pass) & 1, L.split, fresh && pass == 0, fresh);
+      }
   };
   if (reverse) {
     for (int a = 3; a-- > 0;)
@@ -763,15 +789,15 @@ void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter,
   }
   DeviceLevel<T>& F = levels[level];
   DeviceLevel<T>& C = levels[level + 1];
-  smooth(levels, level, policy_.pre_sweeps, false);
+  smooth(levels, level, policy_.pre_sweeps, false, x_zero);
   // Retained defect + restrict_residual in one pass.
   launch_defect_restrict<T>(stream_, F.view(neumann_), F.x, F.b, C.view(neumann_),
-                            C.b, C.x, F.coarsen_mask);
+                            C.b, C.x, F.coarsen_mask, F.split);
   cycle(levels, level + 1, counter, true);
   if (counter > 1) cycle(levels, level + 1, counter - 1, false);
   launch_prolongate<T>(stream_, F.view(neumann_), F.x, C.view(neumann_), C.x,
-                       F.coarsen_mask);
-  smooth(levels, level, policy_.post_sweeps, true);
+                       F.coarsen_mask, F.split);
+  smooth(levels, level, policy_.post_sweeps, true, false);
 }
 
 // NativeCartesianMgPlan::apply_impl (src/solver_mg.cpp:4814-5122).
@@ -783,19 +809,23 @@ void Solver::mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
   for (auto& L : levels) saved.emplace_back(L.x, L.t);
   DeviceLevel<T>& L0 = levels[0];
   const int n = L0.cells();
-  launch_mg_enter<T>(stream_, n, r, d_active_, L0.b, L0.x);
+  const VecLayout v0{L0.nx, L0.ny, L0.split};
+  // x = 0 is written here unless the diagonal shortcut or the first
+  // pre-smoothing sweep (zero flags) defines every entry anyway.
+  const bool zero_x = !(diagonal_shortcut_ || first_sweep_zero_);
+  launch_mg_enter<T>(stream_, n, r, d_active_, L0.b, L0.x, v0, zero_x);
   if (diagonal_shortcut_) {
-    launch_diagonal_solve<T>(stream_, n, L0.b, L0.diag, L0.x);
+    launch_diagonal_solve<T>(stream_, n, L0.b, L0.diag, L0.x, v0);
   } else {
     cycle(levels, 0, policy_.cycle == 1 ? 2 : 1, true);
   }
   if (policy_.unit_linear) {
-    launch_mg_exit<T>(stream_, n, L0.x, d_active_, nullptr, z);
+    launch_mg_exit<T>(stream_, n, L0.x, d_active_, nullptr, z, v0);
   } else {
-    launch_level_defect<T>(stream_, L0.view(neumann_), L0.x, L0.b, L0.r);
+    launch_level_defect<T>(stream_, L0.view(neumann_), L0.x, L0.b, L0.r, L0.split);
     launch_mg_projection<T>(stream_, n, r, d_active_, L0.r,
                             Reduce{d_scalars_, d_partials_, 5});
-    launch_mg_exit<T>(stream_, n, L0.x, d_active_, &d_scalars_->mg_alpha, z);
+    launch_mg_exit<T>(stream_, n, L0.x, d_active_, &d_scalars_->mg_alpha, z, v0);
   }
   for (size_t l = 0; l < levels.size(); ++l) {
     levels[l].x = saved[l].first;
@@ -1879,7 +1909,7 @@ Status Solver::profile_kernel(int kernel, int repetitions, double* ms,
     if (L.line_mask != 0) {
       int axis = 0;
       while (!(L.line_mask & (1 << axis))) ++axis;
-      launch_line_pass<T>(stream_, view, L.x, L.b, L.lfac[axis], L.r, axis, 0);
+      launch_line_pass<T>(stream_, view, L.x, L.b, L.lfac[axis], L.r, axis, 0, L.split);
       return 28.0 / 8.0 * sizeof(T);
     }
     if (L.chebyshev) {
@@ -1907,12 +1937,12 @@ Status Solver::profile_kernel(int kernel, int repetitions, double* ms,
         break;
       case HFPS_KERNEL_RESTRICT_FP64:
         launch_defect_restrict<double>(stream_, A, L0.x, L0.b, l64_[1].view(neumann_),
-                                       l64_[1].b, l64_[1].x, L0.coarsen_mask);
+                                       l64_[1].b, l64_[1].x, L0.coarsen_mask, L0.split);
         per_cell = 48.0 + 2.0 * 8.0 / (l64_[0].cells() / static_cast<double>(l64_[1].cells()));
         break;
       case HFPS_KERNEL_PROLONG_FP64:
         launch_prolongate<double>(stream_, A, L0.x, l64_[1].view(neumann_), l64_[1].x,
-                                  L0.coarsen_mask);
+                                  L0.coarsen_mask, L0.split);
         per_cell = 16.0 + 1.0 + 8.0 / (l64_[0].cells() / static_cast<double>(l64_[1].cells()));
         break;
       case HFPS_KERNEL_PCG_UPDATE:

@@ -38,6 +38,9 @@ struct DeviceLevel {
   T* t{};
   // Line-relaxation factors per strong axis (kernels_line.cu), or null.
   T* lfac[3]{};
+  // Layout of x and b (VecLayout::hx): 0 natural, else split rows with
+  // halves of `split` cells (the finest level of a y- or z-line hierarchy).
+  int split{};
   int cells() const { return nx * ny * nz; }
   int faces_x() const { return (nx + 1) * ny * nz; }
   int faces_y() const { return nx * (ny + 1) * nz; }
@@ -107,7 +110,7 @@ class Solver {
   void cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter, bool x_zero);
   template <class T>
   void smooth(std::vector<DeviceLevel<T>>& levels, int level, int sweeps,
-              bool reverse);
+              bool reverse, bool x_zero);
   template <class T>
   void coarse_solve(std::vector<DeviceLevel<T>>& levels, bool x_zero);
   Status krylov_pcg(const hfps_control& control, hfps_result& result,
@@ -155,6 +158,9 @@ class Solver {
   bool coefficients_ready_{};
   bool mixed_ready_{};
   bool diagonal_shortcut_{};
+  // The finest level's first pre-smoothing sweep runs on the chunked scan
+  // with the zero flags, so the MG entry need not clear x.
+  bool first_sweep_zero_{};
   // Coarsest level in line mode with one line axis and at most
   // kCoarseDenseMaxCells cells: its coarse_sweeps zebra line sweeps are an
   // affine map x_out = P x_in + M b, recorded column by column after every
