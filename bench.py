@@ -281,9 +281,10 @@ def run_reference(args, world, rank):
 
 
 # DRAM bytes per level-0 cell of one zebra colour pass of the FP64 line
-# kernel, from one ncu capture at 256x256x128 (377.8 MB read + 48.2 MB
-# written over 8,388,608 cells); traffic grows with the cell count.
-LINE_PASS_DRAM_BYTES_PER_CELL = (377.820672e6 + 48.243456e6) / (256 * 256 * 128)
+# kernel (split-row vectors, a pass that reads x), from one ncu capture at
+# 256x256x128 (337.1 MB read + 26.1 MB written over 8,388,608 cells);
+# traffic grows with the cell count.
+LINE_PASS_DRAM_BYTES_PER_CELL = (337.118720e6 + 26.119936e6) / (256 * 256 * 128)
 
 # Iterations the reference solve_pcg (production MG, unit_linear) needs per
 # warm-started solve of this workload: 41, 41, 41 for steps 1-3, measured by
@@ -414,7 +415,8 @@ def run_b200(args, world, rank, local):
         peak, peak_note = 6650.0, "fallback"
     dom = kernels["smooth_fp64"]
     roofline = {"bound": "hbm",
-                "kernel": "k_line_scan_color<double,y,8> level 0 (one zebra colour)",
+                "kernel": "k_line_scan_color<double,y,8,normal,split rows> level 0 "
+                          "(one zebra colour)",
                 "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": dom["gbs"] / peak, "peak_source": peak_note,
                 "traffic": LINE_PASS_DRAM_BYTES_PER_CELL * n,
