@@ -275,32 +275,30 @@ __global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
   }
 }
 
-// Trilinear prolongation and add, zero on solid cells (prolongate_cell):
-// one fine vector entry per thread (natural order, or split rows walked
-// entry by entry so that stores stay contiguous), the coarse correction
-// through the read-only path.
-template <class T>
-__global__ void k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C,
-                             const T* __restrict__ cx, int mask, int hx) {
+// Trilinear prolongation and add, zero on solid cells (prolongate_cell).
+// One block per fine x-row (blockIdx.x; blockIdx.y splits long rows), one
+// vector entry per thread (natural order, or split rows walked entry by
+// entry so that stores stay contiguous), the coarse correction through the
+// read-only path, the coarsening mask fixed at compile time.
+constexpr int kProlongThreads = 128;
+
+template <class T, int MASK>
+__global__ void __launch_bounds__(kProlongThreads)
+    k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C, const T* __restrict__ cx, int hx) {
   grid_dependency_sync();
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  int i, j, k, c;
-  if (hx == 0) {
-    c = p;
-    if (c >= F.nx * F.ny * F.nz) return;
-    cell_coords(c, F.nx, F.ny, i, j, k);
-  } else {
-    const int row = p / (2 * hx);
-    if (row >= F.ny * F.nz) return;
-    const int w = p - row * 2 * hx;
+  const int row = blockIdx.x;
+  const int w = blockIdx.y * kProlongThreads + threadIdx.x;
+  int i = w;
+  if (hx != 0) {
     const int odd = w >= hx ? 1 : 0;
     i = 2 * (w - odd * hx) + odd;
-    if (i >= F.nx) return;  // the odd half's padding slot
-    k = row / F.ny;
-    j = row - k * F.ny;
-    c = i + F.nx * row;
   }
-  x[p] = prolongate_cell<T, PlainLoad, RoLoad>(F, x, C, cx, mask, c, i, j, k, p);
+  if (i >= F.nx || (hx != 0 && w >= 2 * hx)) return;  // past the row (or the odd half's padding)
+  const int k = row / F.ny;
+  const int j = row - k * F.ny;
+  const int c = i + F.nx * row;
+  const int at = hx == 0 ? c : 2 * hx * row + w;
+  x[at] = prolongate_cell<T, PlainLoad, RoLoad, MASK>(F, x, C, cx, MASK, c, i, j, k, at);
 }
 
 // Coarsest level: `sweeps` smoother sweeps in one CTA (mg_cycle coarse
@@ -1258,10 +1256,17 @@ void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int mask, int hx) {
-  const long long entries =
-      hx == 0 ? HFPS_CELLS(F) : 2LL * hx * F.ny * static_cast<long long>(F.nz);
-  launch(k_prolongate<T>, static_cast<int>((entries + kThreads - 1) / kThreads), kThreads, 0, s,
-         F, x, C, cx, mask, hx);
+  const int row = hx == 0 ? F.nx : 2 * hx;
+  const dim3 grid(F.ny * F.nz, (row + kProlongThreads - 1) / kProlongThreads);
+  switch (mask & 7) {
+#define HFPS_PROLONG_CASE(M)                                                              \
+  case M:                                                                                 \
+    launch(k_prolongate<T, M>, grid, kProlongThreads, 0, s, F, x, C, cx, hx); \
+    break;
+    HFPS_PROLONG_CASE(0) HFPS_PROLONG_CASE(1) HFPS_PROLONG_CASE(2) HFPS_PROLONG_CASE(3)
+    HFPS_PROLONG_CASE(4) HFPS_PROLONG_CASE(5) HFPS_PROLONG_CASE(6) HFPS_PROLONG_CASE(7)
+#undef HFPS_PROLONG_CASE
+  }
 }
 template <class T, class TC>
 void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,

@@ -266,11 +266,14 @@ __device__ __forceinline__ void interp_axis(int fine, int coarsened,
 // are added in the reference's order (z outer, x inner) with the absent
 // ones skipped by selects, so all loads of a cell are in flight together.
 // LdC reads the coarse correction; the cell's x sits at x[at].
-template <class T, class Ld = PlainLoad, class LdC = PlainLoad>
+// MASK >= 0 fixes the coarsening mask at compile time, so the terms of an
+// axis that is not coarsened (and their loads) drop out.
+template <class T, class Ld = PlainLoad, class LdC = PlainLoad, int MASK = -1>
 __device__ __forceinline__ T prolongate_cell(const Level<T>& F, const T* x, const Level<T>& C,
                                              const T* cx, int mask, int c, int i, int j, int k,
                                              int at) {
-  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
+  const int m = MASK >= 0 ? MASK : mask;
+  const int mx = m & 1, my = (m >> 1) & 1, mz = (m >> 2) & 1;
   const bool fluid = F.fluid[c] != 0;
   const T old = Ld::get(x + at);
   int xi[2], yi[2], zi[2];
