@@ -18,6 +18,14 @@ namespace hfps {
 namespace {
 
 constexpr int kThreads = 256;
+// Row-per-block kernels (transfers): at most this many threads per block,
+// fewer (a multiple of 32) for short rows.
+constexpr int kRowThreads = 128;
+
+dim3 row_grid(int rows, int row_length, int& threads) {
+  threads = std::min(kRowThreads, (row_length + 31) / 32 * 32);
+  return dim3(rows, (row_length + threads - 1) / threads);
+}
 constexpr int kMaxReductionBlocks = 148 * 8;
 
 int grid_for(long long items) {
@@ -235,20 +243,26 @@ __device__ void line_thomas(const Level<T>& L, T* x, const T* b, T* work,
 // Fused retained defect + restriction (apply_level_defect followed by
 // restrict_residual, src/solver_mg.cpp:3633-3721): every coarse cell sums
 // the defects of its children in dz, dy, dx order; coarse x is zeroed.
-template <class T>
-__global__ void k_defect_restrict(Level<T> F, const T* __restrict__ x,
-                                  const T* __restrict__ b, Level<T> C,
-                                  T* __restrict__ cb, T* __restrict__ cx,
-                                  int mask, int hx) {
+// Fused defect + restriction: one block per coarse x-row (blockIdx.x;
+// blockIdx.y splits long rows), one coarse cell per thread, the coarsening
+// mask fixed at compile time; coarse x is zeroed.  Fine x and b in layout hx.
+template <class T, int MASK>
+__global__ void __launch_bounds__(kRowThreads)
+    k_defect_restrict(Level<T> F, const T* __restrict__ x, const T* __restrict__ b, Level<T> C,
+                      T* __restrict__ cb, T* __restrict__ cx, int hx) {
   grid_dependency_sync();
-  const int n = C.nx * C.ny * C.nz;
-  const SplitPos sp{F.ny, hx};
-  for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
-       cc += gridDim.x * blockDim.x) {
-    cb[cc] = hx == 0 ? defect_restrict_cell<T>(F, x, b, C, mask, cc)
-                     : defect_restrict_cell<T, PlainLoad, SplitPos>(F, x, b, C, mask, cc, sp);
-    cx[cc] = T(0);
-  }
+  const int row = blockIdx.x;
+  const int ci = blockIdx.y * blockDim.x + threadIdx.x;
+  if (ci >= C.nx) return;
+  const int ck = row / C.ny;
+  const int cj = row - ck * C.ny;
+  const int cc = ci + C.nx * row;
+  cb[cc] = hx == 0
+               ? defect_restrict_at<T, PlainLoad, NaturalPos, MASK>(F, x, b, MASK, ci, cj, ck,
+                                                                   NaturalPos())
+               : defect_restrict_at<T, PlainLoad, SplitPos, MASK>(F, x, b, MASK, ci, cj, ck,
+                                                                 SplitPos{F.ny, hx});
+  cx[cc] = T(0);
 }
 
 template <class T>
@@ -280,14 +294,12 @@ __global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
 // vector entry per thread (natural order, or split rows walked entry by
 // entry so that stores stay contiguous), the coarse correction through the
 // read-only path, the coarsening mask fixed at compile time.
-constexpr int kProlongThreads = 128;
-
 template <class T, int MASK>
-__global__ void __launch_bounds__(kProlongThreads)
+__global__ void __launch_bounds__(kRowThreads)
     k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C, const T* __restrict__ cx, int hx) {
   grid_dependency_sync();
   const int row = blockIdx.x;
-  const int w = blockIdx.y * kProlongThreads + threadIdx.x;
+  const int w = blockIdx.y * blockDim.x + threadIdx.x;
   int i = w;
   if (hx != 0) {
     const int odd = w >= hx ? 1 : 0;
@@ -1245,8 +1257,17 @@ template <class T>
 void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
                             const T* b, const Level<T>& C, T* cb, T* cx,
                             int mask, int hx) {
-  launch(k_defect_restrict<T>, grid_for(HFPS_CELLS(C)), kThreads, 0, s, F, x, b, C, cb,
-                                                                   cx, mask, hx);
+  int threads = 0;
+  const dim3 grid = row_grid(C.ny * C.nz, C.nx, threads);
+  switch (mask & 7) {
+#define HFPS_RESTRICT_CASE(M)                                                              \
+  case M:                                                                                  \
+    launch(k_defect_restrict<T, M>, grid, threads, 0, s, F, x, b, C, cb, cx, hx);          \
+    break;
+    HFPS_RESTRICT_CASE(0) HFPS_RESTRICT_CASE(1) HFPS_RESTRICT_CASE(2) HFPS_RESTRICT_CASE(3)
+    HFPS_RESTRICT_CASE(4) HFPS_RESTRICT_CASE(5) HFPS_RESTRICT_CASE(6) HFPS_RESTRICT_CASE(7)
+#undef HFPS_RESTRICT_CASE
+  }
 }
 template <class T>
 void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
@@ -1256,12 +1277,12 @@ void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int mask, int hx) {
-  const int row = hx == 0 ? F.nx : 2 * hx;
-  const dim3 grid(F.ny * F.nz, (row + kProlongThreads - 1) / kProlongThreads);
+  int threads = 0;
+  const dim3 grid = row_grid(F.ny * F.nz, hx == 0 ? F.nx : 2 * hx, threads);
   switch (mask & 7) {
 #define HFPS_PROLONG_CASE(M)                                                              \
   case M:                                                                                 \
-    launch(k_prolongate<T, M>, grid, kProlongThreads, 0, s, F, x, C, cx, hx); \
+    launch(k_prolongate<T, M>, grid, threads, 0, s, F, x, C, cx, hx);                     \
     break;
     HFPS_PROLONG_CASE(0) HFPS_PROLONG_CASE(1) HFPS_PROLONG_CASE(2) HFPS_PROLONG_CASE(3)
     HFPS_PROLONG_CASE(4) HFPS_PROLONG_CASE(5) HFPS_PROLONG_CASE(6) HFPS_PROLONG_CASE(7)

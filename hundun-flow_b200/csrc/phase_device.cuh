@@ -208,16 +208,16 @@ __device__ __forceinline__ void chebyshev_cell(const Level<T>& L, const T* x, co
 // ---------------------------------------------------------------------------
 // Transfers (kernels.cu).
 
-// Retained defect + restriction at coarse cell cc (apply_level_defect
-// followed by restrict_residual, src/solver_mg.cpp:3633-3721): the defects
-// of the children summed in dz, dy, dx order.
-template <class T, class Ld = PlainLoad, class Pos = NaturalPos>
-__device__ __forceinline__ T defect_restrict_cell(const Level<T>& F, const T* x, const T* b,
-                                                  const Level<T>& C, int mask, int cc,
-                                                  Pos pos = Pos()) {
-  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
-  int ci, cj, ck;
-  cell_coords(cc, C.nx, C.ny, ci, cj, ck);
+// Retained defect + restriction at coarse cell (ci, cj, ck)
+// (apply_level_defect followed by restrict_residual, src/solver_mg.cpp:
+// 3633-3721): the defects of the children summed in dz, dy, dx order.
+// MASK >= 0 fixes the coarsening mask at compile time (the child loops then
+// unroll, in the same order).
+template <class T, class Ld = PlainLoad, class Pos = NaturalPos, int MASK = -1>
+__device__ __forceinline__ T defect_restrict_at(const Level<T>& F, const T* x, const T* b,
+                                                int mask, int ci, int cj, int ck, Pos pos) {
+  const int m = MASK >= 0 ? MASK : mask;
+  const int mx = m & 1, my = (m >> 1) & 1, mz = (m >> 2) & 1;
   const int xb = mx ? 2 * ci : ci, yb = my ? 2 * cj : cj, zb = mz ? 2 * ck : ck;
   T sum = T(0);
   for (int dz = 0; dz <= mz; ++dz)
