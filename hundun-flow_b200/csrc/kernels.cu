@@ -112,6 +112,23 @@ __device__ __forceinline__ int vec_pos(const VecLayout& v, int c) {
   return 2 * v.hx * row + (i & 1) * v.hx + (i >> 1);
 }
 
+// Calls f(i, j, k, c) for every cell of an nx x ny x nz level: one warp per
+// x-row (rows spread over all warps of the grid), lanes along the row, so
+// loads are contiguous and the row's j, k are formed once per row.
+template <class F>
+__device__ __forceinline__ void for_each_cell_by_rows(int nx, int ny, int nz, F f) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int rows = ny * nz;
+  for (int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); row < rows; row += warps) {
+    const int k = row / ny;
+    const int j = row - k * ny;
+    const int base = nx * row;
+#pragma unroll 4
+    for (int i = lane; i < nx; i += 32) f(i, j, k, base + i);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Level operators: apply_level_matrix / apply_level_defect
 // (src/solver_mg.cpp:2569-2767).
@@ -436,16 +453,12 @@ __global__ void k_mg_projection(int n, const double* __restrict__ r_in,
 __global__ void k_spmv_dot(Level<double> L, const double* __restrict__ x,
                            double* __restrict__ y, Reduce red) {
   grid_dependency_sync();
-  const int n = L.nx * L.ny * L.nz;
   double v[1] = {0.0};
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
-    int i, j, k;
-    cell_coords(c, L.nx, L.ny, i, j, k);
+  for_each_cell_by_rows(L.nx, L.ny, L.nz, [&](int i, int j, int k, int c) {
     const double a = row_value(L, x, i, j, k, c);
     y[c] = a;
     v[0] += x[c] * a;
-  }
+  });
   if (finish_reduction<1>(v, red) && threadIdx.x == 0)
     apply_scalar_op(red.scalars, red.op, v[0]);
 }
@@ -454,16 +467,12 @@ __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
                                 const double* __restrict__ b,
                                 double* __restrict__ r, Reduce red) {
   grid_dependency_sync();
-  const int n = L.nx * L.ny * L.nz;
   double v[1] = {0.0};
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
-    int i, j, k;
-    cell_coords(c, L.nx, L.ny, i, j, k);
+  for_each_cell_by_rows(L.nx, L.ny, L.nz, [&](int i, int j, int k, int c) {
     const double value = b[c] - row_value(L, x, i, j, k, c);
     r[c] = value;
     v[0] += value * value;
-  }
+  });
   if (finish_reduction<1>(v, red) && threadIdx.x == 0)
     apply_scalar_op(red.scalars, red.op, v[0]);
 }
@@ -637,14 +646,10 @@ __global__ void k_operator_shift(Level<double> L, const double* __restrict__ z,
                                  const double* __restrict__ v, double shift,
                                  double* __restrict__ w) {
   grid_dependency_sync();
-  const int n = L.nx * L.ny * L.nz;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
-    int i, j, k;
-    cell_coords(c, L.nx, L.ny, i, j, k);
+  for_each_cell_by_rows(L.nx, L.ny, L.nz, [&](int i, int j, int k, int c) {
     const double a = row_value(L, z, i, j, k, c);
     w[c] = a + -shift * v[c];
-  }
+  });
 }
 
 // Up to kBasisChunk dot products v_r . w (and w . w when `self`), one pass
