@@ -266,14 +266,14 @@ __device__ void line_thomas(const Level<T>& L, T* x, const T* b, T* work,
 template <class T, int MASK>
 __global__ void __launch_bounds__(kRowThreads)
     k_defect_restrict(Level<T> F, const T* __restrict__ x, const T* __restrict__ b, Level<T> C,
-                      T* __restrict__ cb, T* __restrict__ cx, int hx) {
+                      T* __restrict__ cb, T* __restrict__ cx, int hx, int hxc) {
   grid_dependency_sync();
   const int row = blockIdx.x;
   const int ci = blockIdx.y * blockDim.x + threadIdx.x;
   if (ci >= C.nx) return;
   const int ck = row / C.ny;
   const int cj = row - ck * C.ny;
-  const int cc = ci + C.nx * row;
+  const int cc = hxc == 0 ? ci + C.nx * row : SplitPos{C.ny, hxc}(0, ci, cj, ck);
   cb[cc] = hx == 0
                ? defect_restrict_at<T, PlainLoad, NaturalPos, MASK>(F, x, b, MASK, ci, cj, ck,
                                                                    NaturalPos())
@@ -313,7 +313,8 @@ __global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
 // read-only path, the coarsening mask fixed at compile time.
 template <class T, int MASK>
 __global__ void __launch_bounds__(kRowThreads)
-    k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C, const T* __restrict__ cx, int hx) {
+    k_prolongate(Level<T> F, T* __restrict__ x, Level<T> C, const T* __restrict__ cx, int hx,
+                 int hxc) {
   grid_dependency_sync();
   const int row = blockIdx.x;
   const int w = blockIdx.y * blockDim.x + threadIdx.x;
@@ -327,7 +328,9 @@ __global__ void __launch_bounds__(kRowThreads)
   const int j = row - k * F.ny;
   const int c = i + F.nx * row;
   const int at = hx == 0 ? c : 2 * hx * row + w;
-  x[at] = prolongate_cell<T, PlainLoad, RoLoad, MASK>(F, x, C, cx, MASK, c, i, j, k, at);
+  x[at] = hxc == 0 ? prolongate_cell<T, PlainLoad, RoLoad, MASK>(F, x, C, cx, MASK, c, i, j, k, at)
+                   : prolongate_cell<T, PlainLoad, RoLoad, MASK, SplitPos>(
+                         F, x, C, cx, MASK, c, i, j, k, at, SplitPos{C.ny, hxc});
 }
 
 // Coarsest level: `sweeps` smoother sweeps in one CTA (mg_cycle coarse
@@ -1261,13 +1264,13 @@ void launch_chebyshev_stage(cudaStream_t s, const Level<T>& L, const T* x,
 template <class T>
 void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
                             const T* b, const Level<T>& C, T* cb, T* cx,
-                            int mask, int hx) {
+                            int mask, int hx, int hxc) {
   int threads = 0;
   const dim3 grid = row_grid(C.ny * C.nz, C.nx, threads);
   switch (mask & 7) {
 #define HFPS_RESTRICT_CASE(M)                                                              \
   case M:                                                                                  \
-    launch(k_defect_restrict<T, M>, grid, threads, 0, s, F, x, b, C, cb, cx, hx);          \
+    launch(k_defect_restrict<T, M>, grid, threads, 0, s, F, x, b, C, cb, cx, hx, hxc);     \
     break;
     HFPS_RESTRICT_CASE(0) HFPS_RESTRICT_CASE(1) HFPS_RESTRICT_CASE(2) HFPS_RESTRICT_CASE(3)
     HFPS_RESTRICT_CASE(4) HFPS_RESTRICT_CASE(5) HFPS_RESTRICT_CASE(6) HFPS_RESTRICT_CASE(7)
@@ -1281,13 +1284,13 @@ void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
 }
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
-                       const Level<T>& C, const T* cx, int mask, int hx) {
+                       const Level<T>& C, const T* cx, int mask, int hx, int hxc) {
   int threads = 0;
   const dim3 grid = row_grid(F.ny * F.nz, hx == 0 ? F.nx : 2 * hx, threads);
   switch (mask & 7) {
 #define HFPS_PROLONG_CASE(M)                                                              \
   case M:                                                                                 \
-    launch(k_prolongate<T, M>, grid, threads, 0, s, F, x, C, cx, hx);                     \
+    launch(k_prolongate<T, M>, grid, threads, 0, s, F, x, C, cx, hx, hxc);                \
     break;
     HFPS_PROLONG_CASE(0) HFPS_PROLONG_CASE(1) HFPS_PROLONG_CASE(2) HFPS_PROLONG_CASE(3)
     HFPS_PROLONG_CASE(4) HFPS_PROLONG_CASE(5) HFPS_PROLONG_CASE(6) HFPS_PROLONG_CASE(7)
@@ -1510,11 +1513,11 @@ void launch_adjoint_source(cudaStream_t s, int n, const double* dl_dp,
                                           const T*, T*, T*, T, T, int);            \
   template void launch_defect_restrict<T>(cudaStream_t, const Level<T>&, const T*, \
                                           const T*, const Level<T>&, T*, T*, int,  \
-                                          int);                                    \
+                                          int, int);                               \
   template void launch_restrict<T>(cudaStream_t, const Level<T>&, const T*,        \
                                    const Level<T>&, T*, T*, int);                  \
   template void launch_prolongate<T>(cudaStream_t, const Level<T>&, T*,            \
-                                     const Level<T>&, const T*, int, int);         \
+                                     const Level<T>&, const T*, int, int, int);    \
   template void launch_mg_enter<T>(cudaStream_t, int, const double*,               \
                                    const uint8_t*, T*, T*, VecLayout, bool);       \
   template void launch_mg_exit<T>(cudaStream_t, int, const T*, const uint8_t*,     \

@@ -75,17 +75,19 @@ template <class T>
 void launch_chebyshev_stage(cudaStream_t s, const Level<T>& L, const T* x,
                             const T* b, T* direction, T* next,
                             T previous_factor, T residual_factor, int first);
-// Fine x, b in layout hx; coarse vectors natural.
+// Fine x, b in layout hx, coarse b, x in layout hxc.
 template <class T>
 void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
                             const T* b, const Level<T>& C, T* cb, T* cx,
-                            int coarsen_mask, int hx = 0);
+                            int coarsen_mask, int hx = 0, int hxc = 0);
 template <class T>
 void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
                      const Level<T>& C, T* cb, T* cx, int coarsen_mask);
+// Fine x in layout hx, coarse x in layout hxc.
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
-                       const Level<T>& C, const T* cx, int coarsen_mask, int hx = 0);
+                       const Level<T>& C, const T* cx, int coarsen_mask, int hx = 0,
+                       int hxc = 0);
 // ---- zebra line relaxation (kernels_line.cu) --------------------------------
 // Line-colour passes with more lines than this run the chunked-scan solve
 // (lanes across lines, warps along chunks of one line); fewer lines run PCR

@@ -265,13 +265,15 @@ __device__ __forceinline__ void interp_axis(int fine, int coarsened,
 // unconditionally (a degenerate axis repeats its one index) and the terms
 // are added in the reference's order (z outer, x inner) with the absent
 // ones skipped by selects, so all loads of a cell are in flight together.
-// LdC reads the coarse correction; the cell's x sits at x[at].
+// LdC reads the coarse correction, which is stored in layout CPos; the
+// cell's x sits at x[at].
 // MASK >= 0 fixes the coarsening mask at compile time, so the terms of an
 // axis that is not coarsened (and their loads) drop out.
-template <class T, class Ld = PlainLoad, class LdC = PlainLoad, int MASK = -1>
+template <class T, class Ld = PlainLoad, class LdC = PlainLoad, int MASK = -1,
+          class CPos = NaturalPos>
 __device__ __forceinline__ T prolongate_cell(const Level<T>& F, const T* x, const Level<T>& C,
                                              const T* cx, int mask, int c, int i, int j, int k,
-                                             int at) {
+                                             int at, CPos cpos = CPos()) {
   const int m = MASK >= 0 ? MASK : mask;
   const int mx = m & 1, my = (m >> 1) & 1, mz = (m >> 2) & 1;
   const bool fluid = F.fluid[c] != 0;
@@ -293,7 +295,9 @@ __device__ __forceinline__ T prolongate_cell(const Level<T>& F, const T* x, cons
         const double wy = ay == 0 ? 1.0 - yw : yw;
         const double wx = ax == 0 ? 1.0 - xw : xw;
         const T w = static_cast<T>(wx * wy * wz);
-        term[az][ay][ax] = w * LdC::get(cx + xi[ax] + C.nx * (yi[ay] + C.ny * zi[az]));
+        term[az][ay][ax] =
+            w * LdC::get(cx + cpos(xi[ax] + C.nx * (yi[ay] + C.ny * zi[az]), xi[ax], yi[ay],
+                                   zi[az]));
       }
   T value = T(0);
 #pragma unroll

@@ -219,18 +219,21 @@ Status Solver::allocate() {
       if ((s.line_mask & (1 << a)) && line_kind(s.n[0], s.n[1], s.n[2], a) == kLineNone)
         return fail(HFPS_INVALID_PLAN, kDetailPlan, "line relaxation: line longer than 2048 cells");
   const int levels = static_cast<int>(shapes.size());
-  // Split rows for the finest level's MG x and b when it relaxes y- or
-  // z-lines with the chunked scan: a colour pass then reads and writes whole
-  // halves of rows instead of every other cell (HFPS_SPLIT0=0 keeps the
-  // natural order).
-  int split0 = 0;
+  // Split rows for the MG x and b of every non-coarsest level that relaxes
+  // y- or z-lines with the chunked scan: a colour pass then reads and writes
+  // whole halves of rows instead of every other cell (HFPS_SPLIT_ROWS=0 keeps
+  // the natural order).
+  std::vector<int> split(levels, 0);
   {
-    const Shape& s0 = shapes[0];
-    const char* env = std::getenv("HFPS_SPLIT0");
-    const int axis = s0.line_mask == 2 ? 1 : (s0.line_mask == 4 ? 2 : -1);
-    const bool scan = axis > 0 && line_kind(s0.n[0], s0.n[1], s0.n[2], axis) == kLineScan;
-    if (scan && !(env != nullptr && env[0] == '0')) split0 = (s0.n[0] + 1) / 2;
-    first_sweep_zero_ = scan && policy_.pre_sweeps >= 1;
+    const char* env = std::getenv("HFPS_SPLIT_ROWS");
+    const bool on = !(env != nullptr && env[0] == '0');
+    for (int l = 0; l + 1 < levels; ++l) {
+      const Shape& sl = shapes[l];
+      const int axis = sl.line_mask == 2 ? 1 : (sl.line_mask == 4 ? 2 : -1);
+      const bool scan = axis > 0 && line_kind(sl.n[0], sl.n[1], sl.n[2], axis) == kLineScan;
+      if (scan && on) split[l] = (sl.n[0] + 1) / 2;
+      if (l == 0) first_sweep_zero_ = scan && policy_.pre_sweeps >= 1;
+    }
   }
   // Sizes.
   size_t bytes = 0;
@@ -255,9 +258,7 @@ Status Solver::allocate() {
     max_faces = std::max({max_faces, fx, fy, fz});
     Offsets& o = off[l];
     // x and b hold 2 * hx * ny * nz values in split rows.
-    const size_t cv = l == 0 && split0 > 0
-                          ? 2 * static_cast<size_t>(split0) * s.n[1] * s.n[2]
-                          : c;
+    const size_t cv = split[l] > 0 ? 2 * static_cast<size_t>(split[l]) * s.n[1] * s.n[2] : c;
     o.d = add(c * 8); o.fx = add(fx * 8); o.fy = add(fy * 8); o.fz = add(fz * 8);
     o.x = add(cv * 8); o.b = add(cv * 8); o.r = add(c * 8); o.t = add(c * 8);
     o.vol = add(c * 8); o.fluid = add(c);
@@ -362,7 +363,7 @@ Status Solver::allocate() {
     a.nz = b.nz = s.n[2];
     a.coarsen_mask = b.coarsen_mask = s.coarsen_mask;
     a.line_mask = b.line_mask = s.line_mask;
-    a.split = b.split = l == 0 ? split0 : 0;
+    a.split = b.split = split[l];
     // build_levels: Chebyshev only on non-coarsest point levels
     // (src/solver_mg.cpp:1060-1073).
     a.chebyshev = b.chebyshev =
@@ -792,11 +793,11 @@ void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter,
   smooth(levels, level, policy_.pre_sweeps, false, x_zero);
   // Retained defect + restrict_residual in one pass.
   launch_defect_restrict<T>(stream_, F.view(neumann_), F.x, F.b, C.view(neumann_),
-                            C.b, C.x, F.coarsen_mask, F.split);
+                            C.b, C.x, F.coarsen_mask, F.split, C.split);
   cycle(levels, level + 1, counter, true);
   if (counter > 1) cycle(levels, level + 1, counter - 1, false);
   launch_prolongate<T>(stream_, F.view(neumann_), F.x, C.view(neumann_), C.x,
-                       F.coarsen_mask, F.split);
+                       F.coarsen_mask, F.split, C.split);
   smooth(levels, level, policy_.post_sweeps, true, false);
 }
 
@@ -1937,12 +1938,13 @@ Status Solver::profile_kernel(int kernel, int repetitions, double* ms,
         break;
       case HFPS_KERNEL_RESTRICT_FP64:
         launch_defect_restrict<double>(stream_, A, L0.x, L0.b, l64_[1].view(neumann_),
-                                       l64_[1].b, l64_[1].x, L0.coarsen_mask, L0.split);
+                                       l64_[1].b, l64_[1].x, L0.coarsen_mask, L0.split,
+                                       l64_[1].split);
         per_cell = 48.0 + 2.0 * 8.0 / (l64_[0].cells() / static_cast<double>(l64_[1].cells()));
         break;
       case HFPS_KERNEL_PROLONG_FP64:
         launch_prolongate<double>(stream_, A, L0.x, l64_[1].view(neumann_), l64_[1].x,
-                                  L0.coarsen_mask, L0.split);
+                                  L0.coarsen_mask, L0.split, l64_[1].split);
         per_cell = 16.0 + 1.0 + 8.0 / (l64_[0].cells() / static_cast<double>(l64_[1].cells()));
         break;
       case HFPS_KERNEL_PCG_UPDATE:

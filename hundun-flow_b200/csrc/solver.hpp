@@ -39,7 +39,8 @@ struct DeviceLevel {
   // Line-relaxation factors per strong axis (kernels_line.cu), or null.
   T* lfac[3]{};
   // Layout of x and b (VecLayout::hx): 0 natural, else split rows with
-  // halves of `split` cells (the finest level of a y- or z-line hierarchy).
+  // halves of `split` cells (levels of a y- or z-line hierarchy that relax
+  // with the chunked scan).
   int split{};
   int cells() const { return nx * ny * nz; }
   int faces_x() const { return (nx + 1) * ny * nz; }

@@ -1,13 +1,13 @@
-"""Split-row layout of the finest level's MG vectors against the natural order.
+"""Split-row layout of the MG vectors against the natural order.
 
-When the finest level relaxes y- or z-lines with the chunked scan, its MG x
-and b are stored in split rows (each x-row's even-i cells, then its odd-i
-cells), and the first pre-smoothing sweep reads no x instead of the MG entry
-clearing it; HFPS_SPLIT0=0 (read when the solver is created) keeps the natural
-order and the clearing.  Both perform the same operations on the same values,
-so the MG application and whole solves must agree bit for bit: FP64 and
-mixed, unit and residual-minimising corrections, even and odd nx (the odd
-half of a split row then has a padding slot), y- and z-lines.
+On every level that relaxes y- or z-lines with the chunked scan, the MG x and
+b are stored in split rows (each x-row's even-i cells, then its odd-i cells),
+and the first pre-smoothing sweep of the finest level reads no x instead of
+the MG entry clearing it; HFPS_SPLIT_ROWS=0 (read when the solver is created)
+keeps the natural order everywhere.  Both perform the same operations on the
+same values, so the MG application and whole solves must agree bit for bit:
+FP64 and mixed, unit and residual-minimising corrections, even and odd nx
+(the odd half of a split row then has a padding slot), y- and z-lines.
 """
 import os
 
@@ -48,15 +48,15 @@ CASES = {
 
 
 def make_solver(hfps, system, policy, split):
-    saved = os.environ.get("HFPS_SPLIT0")
-    os.environ["HFPS_SPLIT0"] = "1" if split else "0"
+    saved = os.environ.get("HFPS_SPLIT_ROWS")
+    os.environ["HFPS_SPLIT_ROWS"] = "1" if split else "0"
     try:
         return hfps.PressureSolver.from_system(system, policy)
     finally:
         if saved is None:
-            os.environ.pop("HFPS_SPLIT0", None)
+            os.environ.pop("HFPS_SPLIT_ROWS", None)
         else:
-            os.environ["HFPS_SPLIT0"] = saved
+            os.environ["HFPS_SPLIT_ROWS"] = saved
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
