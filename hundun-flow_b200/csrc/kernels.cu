@@ -409,6 +409,26 @@ __global__ void k_mg_exit(int n, const T* __restrict__ x,
   }
 }
 
+// MG exit with the PCG's r.z: z = active ? x : 0 (unit scaling) and the sum
+// of r * z, accumulated in k_dot's order (same grid, same per-thread cells),
+// then red.op.  Replaces k_mg_exit followed by k_dot(r, z).
+template <class T>
+__global__ void k_mg_exit_dot(int n, const T* __restrict__ x,
+                              const uint8_t* __restrict__ active, double* __restrict__ z,
+                              VecLayout v, const double* __restrict__ r, Reduce red) {
+  grid_dependency_sync();
+  double acc[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const bool on = active == nullptr || active[c] != 0;
+    const double zc = on ? static_cast<double>(x[vec_pos(v, c)]) * 1.0 : 0.0;
+    z[c] = zc;
+    acc[0] += r[c] * zc;
+  }
+  if (finish_reduction<1>(acc, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, acc[0]);
+}
+
 template <class T>
 __global__ void k_diagonal_solve(int n, const T* __restrict__ b,
                                  const T* __restrict__ diag,
@@ -1315,6 +1335,11 @@ void launch_mg_exit(cudaStream_t s, int n, const T* x, const uint8_t* active,
   launch(k_mg_exit<T>, grid_for(n), kThreads, 0, s, n, x, active, scale_ptr, z, v);
 }
 template <class T>
+void launch_mg_exit_dot(cudaStream_t s, int n, const T* x, const uint8_t* active, double* z,
+                        VecLayout v, const double* r, Reduce red) {
+  launch(k_mg_exit_dot<T>, reduction_blocks(n), kThreads, 0, s, n, x, active, z, v, r, red);
+}
+template <class T>
 void launch_diagonal_solve(cudaStream_t s, int n, const T* b, const T* diag,
                            T* x, VecLayout v) {
   launch(k_diagonal_solve<T>, grid_for(n), kThreads, 0, s, n, b, diag, x, v);
@@ -1522,6 +1547,8 @@ void launch_adjoint_source(cudaStream_t s, int n, const double* dl_dp,
                                    const uint8_t*, T*, T*, VecLayout, bool);       \
   template void launch_mg_exit<T>(cudaStream_t, int, const T*, const uint8_t*,     \
                                   const double*, double*, VecLayout);              \
+  template void launch_mg_exit_dot<T>(cudaStream_t, int, const T*, const uint8_t*, \
+                                      double*, VecLayout, const double*, Reduce);  \
   template void launch_diagonal_solve<T>(cudaStream_t, int, const T*, const T*,    \
                                          T*, VecLayout);                           \
   template void launch_mg_projection<T>(cudaStream_t, int, const double*,          \

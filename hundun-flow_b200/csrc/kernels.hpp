@@ -142,6 +142,10 @@ void launch_mg_enter(cudaStream_t s, int n, const double* r,
 template <class T>
 void launch_mg_exit(cudaStream_t s, int n, const T* x, const uint8_t* active,
                     const double* scale_ptr, double* z, VecLayout v);
+// launch_mg_exit (unit scaling) fused with the PCG's r.z through red.
+template <class T>
+void launch_mg_exit_dot(cudaStream_t s, int n, const T* x, const uint8_t* active, double* z,
+                        VecLayout v, const double* r, Reduce red);
 template <class T>
 void launch_diagonal_solve(cudaStream_t s, int n, const T* b, const T* diag,
                            T* x, VecLayout v);

@@ -342,6 +342,12 @@ Status Solver::allocate() {
   kp_ = reinterpret_cast<double*>(at(k_off[3]));
   kap_ = reinterpret_cast<double*>(at(k_off[4]));
   kb_ = reinterpret_cast<double*>(at(k_off[5]));
+  {
+    // PCG's r.z formed in the MG exit (HFPS_KRYLOV_FUSION=0 keeps the
+    // separate dot kernel).
+    const char* env = std::getenv("HFPS_KRYLOV_FUSION");
+    krylov_fusion_ = !(env != nullptr && env[0] == '0');
+  }
   d_scalars_ = reinterpret_cast<Scalars*>(at(scalars_off));
   d_partials_ = reinterpret_cast<double*>(at(partials_off));
   coarse_op_ = dense_off == SIZE_MAX ? nullptr : reinterpret_cast<double*>(at(dense_off));
@@ -820,7 +826,12 @@ void Solver::mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
   } else {
     cycle(levels, 0, policy_.cycle == 1 ? 2 : 1, true);
   }
-  if (policy_.unit_linear) {
+  if (policy_.unit_linear && krylov_fusion_) {
+    // The PCG consumes r.z of every preconditioner application: formed here
+    // while z is written (kOpRhoNext; the PCG's restarts use only rho).
+    launch_mg_exit_dot<T>(stream_, n, L0.x, d_active_, z, v0, r,
+                          Reduce{d_scalars_, d_partials_, kOpRhoNext});
+  } else if (policy_.unit_linear) {
     launch_mg_exit<T>(stream_, n, L0.x, d_active_, nullptr, z, v0);
   } else {
     launch_level_defect<T>(stream_, L0.view(neumann_), L0.x, L0.b, L0.r, L0.split);
@@ -949,13 +960,20 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
     result.termination = HFPS_CONVERGED;
     return {};
   }
+  // With the MG preconditioner at unit scaling the MG exit forms r.z itself
+  // (kOpRhoNext: rho = r.z; a restart uses only rho).
+  const bool fused_dot = krylov_fusion_ && policy_.unit_linear &&
+                         policy_.preconditioner != HFPS_PRECONDITIONER_IC0;
   const auto restart_direction = [&]() -> Status {
     Status s = precondition(mixed);
     if (!s) return s;
     ++result.preconditioner_applies;
-    launch_dot(stream_, n, kr_, kz_, red(kOpRhoRestart));
+    if (!fused_dot) {
+      launch_dot(stream_, n, kr_, kz_, red(kOpRhoRestart));
+      launches_ += 1;
+    }
     launch_copy(stream_, n, kz_, kp_);
-    launches_ += 2;
+    launches_ += 1;
     return {};
   };
   st = restart_direction();
@@ -1012,9 +1030,12 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
     st = precondition(mixed);
     if (!st) return st;
     ++result.preconditioner_applies;
-    launch_dot(stream_, n, kr_, kz_, red(kOpRhoNext));
+    if (!fused_dot) {
+      launch_dot(stream_, n, kr_, kz_, red(kOpRhoNext));
+      launches_ += 1;
+    }
     launch_p_update(stream_, n, kp_, kz_, d_scalars_);
-    launches_ += 2;
+    launches_ += 1;
   }
   result.termination = HFPS_MAXIMUM_ITERATIONS;
   return fail(HFPS_REJECTED_STEP, kDetailBreakdown, "maximum iterations reached");

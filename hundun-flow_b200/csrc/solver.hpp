@@ -153,6 +153,7 @@ class Solver {
   double* kp_{};
   double* kap_{};
   double* kb_{};
+  bool krylov_fusion_{true};  // PCG's r.z formed in the MG exit
   Scalars* d_scalars_{};
   Scalars* h_scalars_{};      // pinned
   double* d_partials_{};
