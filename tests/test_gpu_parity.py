@@ -105,6 +105,37 @@ def test_mg_scan_lines_match(hfps_mod, shape):
     assert rel(g.apply_preconditioner(v), o.apply_mg(v)) <= 1e-13
 
 
+def stretched_front(n, axis, ratio=1.05):
+    """A wrinkled density front on a grid stretched along `axis` (0 x, 2 z)."""
+    faces = [workloads.uniform_faces(m) for m in n]
+    faces[axis] = workloads.stretched_faces(n[axis], ratio)
+    faces = tuple(faces)
+    z, y, x = workloads._grid(faces)
+    front = (y - 0.4 - 0.05 * np.sin(8.0 * np.pi * x) * np.sin(8.0 * np.pi * z)) / 0.01
+    rho = workloads._tanh_front(front) * np.ones(n[::-1])
+    solid = np.broadcast_to((x - 0.2) ** 2 + (z - 0.5) ** 2 <= 0.08 * 0.08, n[::-1]).copy()
+    return workloads._build("stretched_front", faces, rho, solid, workloads.PISO_BOUNDARY, 4)
+
+
+@pytest.mark.parametrize("axis,shape", [(0, (96, 64, 48)), (2, (64, 48, 96))])
+def test_mg_scan_lines_other_axes(hfps_mod, axis, shape):
+    """x- and z-line relaxation with the chunked scan (z-lines with split-row
+    vectors) against the restatement's serial Thomas solves."""
+    s = stretched_front(shape, axis)
+    pol = ref_oracle_policy()
+    g = hfps_mod.PressureSolver.from_system(s, gpu_policy(hfps_mod, pol))
+    o = oracle(s, pol, line_order=1)
+    assert o.levels()[0][3] == 1 << axis
+    assert g.levels()[0][3] == 1 << axis
+    v = golden_cases.probe(s)
+    assert rel(g.apply_preconditioner(v), o.apply_mg(v)) <= 1e-13
+
+
+def ref_oracle_policy():
+    import ref_oracle
+    return ref_oracle.MgPolicy(cycle=0, pre=1, post=1, coarse_sweeps=2, max_levels=2)
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_solve_parity_with_reference(hfps_mod, name):
     s = golden_cases.system(name)
