@@ -678,26 +678,28 @@ __global__ void k_operator_shift(Level<double> L, const double* __restrict__ z,
 // Up to kBasisChunk dot products v_r . w (and w . w when `self`), one pass
 // over w; deterministic block partials finished by the last block
 // (local_multidot + checked_sum, :206-244).
+// COUNT basis vectors and SELF fixed at compile time: every load of a cell
+// is unconditional, so they are all in flight together (a runtime count
+// turned them into a chain of branches, each waiting on its load).
+template <int COUNT, bool SELF>
 __global__ void k_multidot(int n, BasisRefs basis, const double* __restrict__ w,
-                           int self, double* __restrict__ out, Reduce red) {
+                           double* __restrict__ out, Reduce red) {
   grid_dependency_sync();
   double acc[kBasisChunk];
 #pragma unroll
   for (int r = 0; r < kBasisChunk; ++r) acc[r] = 0.0;
-  const int count = basis.count;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
     const double wc = w[c];
 #pragma unroll
-    for (int r = 0; r < kBasisChunk; ++r) {
-      if (r < count) acc[r] += __ldg(basis.v[r] + c) * wc;
-      else if (r == count && self) acc[r] += wc * wc;
-    }
+    for (int r = 0; r < COUNT; ++r) acc[r] += __ldg(basis.v[r] + c) * wc;
+    if (SELF) acc[COUNT] += wc * wc;
   }
+  constexpr int kOut = COUNT + (SELF ? 1 : 0);
   if (finish_reduction<kBasisChunk>(acc, red) && threadIdx.x == 0) {
-    for (int r = 0; r < count + (self ? 1 : 0); ++r) out[r] = acc[r];
+    for (int r = 0; r < kOut; ++r) out[r] = acc[r];
     int bad = 0;
-    for (int r = 0; r < count + (self ? 1 : 0); ++r) bad |= !isfinite(acc[r]);
+    for (int r = 0; r < kOut; ++r) bad |= !isfinite(acc[r]);
     if (bad) red.scalars->flags |= 1;
   }
 }
@@ -719,16 +721,15 @@ __global__ void k_difference_nonzero(int n, const double* __restrict__ x,
 // out = scale * (dst + s_0 v_0 + s_1 v_1 + ...), terms added per cell in
 // basis order (add_scaled_basis, :510-564), then optionally scaled
 // (scale_copy, :611-625); `out` may be `dst`.
+template <int COUNT>
 __global__ void k_basis_update(int n, const double* dst, BasisRefs basis,
                                double scale, int scaled, double* out) {
   grid_dependency_sync();
-  const int count = basis.count;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += gridDim.x * blockDim.x) {
     double v = dst[c];
 #pragma unroll
-    for (int r = 0; r < kBasisChunk; ++r)
-      if (r < count) v = v + basis.s[r] * __ldg(basis.v[r] + c);
+    for (int r = 0; r < COUNT; ++r) v = v + basis.s[r] * __ldg(basis.v[r] + c);
     if (scaled) v = scale * v;
     out[c] = v;
   }
@@ -1417,9 +1418,26 @@ void launch_operator_shift(cudaStream_t s, const Level<double>& L, const double*
                            const double* v, double shift, double* w) {
   launch(k_operator_shift, grid_for(HFPS_CELLS(L)), kThreads, 0, s, L, z, v, shift, w);
 }
+#define HFPS_BASIS_COUNTS(X)                                                             \
+  X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
+
 void launch_multidot(cudaStream_t s, int n, const BasisRefs& basis, const double* w,
                      bool self, double* out, Reduce red) {
-  launch(k_multidot, reduction_blocks(n), kThreads, 0, s, n, basis, w, self ? 1 : 0, out, red);
+  const int blocks = reduction_blocks(n);
+  switch (basis.count + (self ? 100 : 0)) {
+#define HFPS_MULTIDOT_CASE(C)                                                              \
+  case C:                                                                                  \
+    launch(k_multidot<C, false>, blocks, kThreads, 0, s, n, basis, w, out, red);            \
+    break;                                                                                 \
+  case 100 + C:                                                                            \
+    if (C < kBasisChunk)                                                                   \
+      launch(k_multidot<(C < kBasisChunk ? C : 0), true>, blocks, kThreads, 0, s, n, basis, \
+             w, out, red);                                                                 \
+    break;
+    HFPS_BASIS_COUNTS(HFPS_MULTIDOT_CASE)
+#undef HFPS_MULTIDOT_CASE
+    default: break;
+  }
 }
 void launch_difference_nonzero(cudaStream_t s, int n, const double* x, double* snap,
                                Scalars* scalars) {
@@ -1427,8 +1445,16 @@ void launch_difference_nonzero(cudaStream_t s, int n, const double* x, double* s
 }
 void launch_basis_update(cudaStream_t s, int n, const double* dst, const BasisRefs& basis,
                          double scale, bool scaled, double* out) {
-  launch(k_basis_update, grid_for(n), kThreads, 0, s, n, dst, basis, scale, scaled ? 1 : 0,
-         out);
+  switch (basis.count) {
+#define HFPS_BASIS_CASE(C)                                                                 \
+  case C:                                                                                  \
+    launch(k_basis_update<C>, grid_for(n), kThreads, 0, s, n, dst, basis, scale,           \
+           scaled ? 1 : 0, out);                                                           \
+    break;
+    HFPS_BASIS_COUNTS(HFPS_BASIS_CASE)
+#undef HFPS_BASIS_CASE
+    default: break;
+  }
 }
 void launch_copy(cudaStream_t s, int n, const double* src, double* dst) {
   launch(k_copy, grid_for(n), kThreads, 0, s, n, src, dst);
