@@ -121,8 +121,7 @@ Status Solver::check(cudaError_t e, const char* what) {
 
 Solver::~Solver() {
   if (stream_ != nullptr) cudaStreamSynchronize(stream_);
-  for (auto& g : mg_graph_)
-    if (g != nullptr) cudaGraphExecDestroy(g);
+  clear_mg_graphs();
   if (dic_graph_ != nullptr) cudaGraphExecDestroy(dic_graph_);
   if (h_scalars_ != nullptr) cudaFreeHost(h_scalars_);
   if (arena_ != nullptr) cudaFree(arena_);
@@ -519,10 +518,7 @@ Status Solver::build_hierarchy() {
   }
   coefficients_ready_ = true;
   mixed_ready_ = false;
-  for (auto& gexec : mg_graph_) {
-    if (gexec != nullptr) cudaGraphExecDestroy(gexec);
-    gexec = nullptr;
-  }
+  clear_mg_graphs();
   st = check(cudaStreamSynchronize(stream_), "hierarchy");
   if (!st) return st;
   return dic_factor();
@@ -845,36 +841,48 @@ void Solver::mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
   }
 }
 
-Status Solver::mg_apply(bool mixed) {
+void Solver::clear_mg_graphs() {
+  for (MgGraph& g : mg_graphs_)
+    if (g.exec != nullptr) cudaGraphExecDestroy(g.exec);
+  mg_graphs_.clear();
+}
+
+Status Solver::mg_apply(bool mixed, const double* r, double* z) {
   if (mixed) {
     Status st = refresh_mixed();
     if (!st) return st;
   }
+  if (r == nullptr) r = kr_;
+  if (z == nullptr) z = kz_;
   const int slot = mixed ? 1 : 0;
   if (!use_graphs_) {
-    if (mixed) mg_enqueue(l32_, kr_, kz_);
-    else mg_enqueue(l64_, kr_, kz_);
+    if (mixed) mg_enqueue(l32_, r, z);
+    else mg_enqueue(l64_, r, z);
     launches_ += mg_nodes_[slot];
     return check(cudaGetLastError(), "mg launch");
   }
-  if (mg_graph_[slot] == nullptr) {
+  cudaGraphExec_t exec = nullptr;
+  for (const MgGraph& g : mg_graphs_)
+    if (g.slot == slot && g.r == r && g.z == z) exec = g.exec;
+  if (exec == nullptr) {
     cudaGraph_t graph = nullptr;
     Status st = check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal),
                       "graph capture begin");
     if (!st) return st;
-    if (mixed) mg_enqueue(l32_, kr_, kz_);
-    else mg_enqueue(l64_, kr_, kz_);
+    if (mixed) mg_enqueue(l32_, r, z);
+    else mg_enqueue(l64_, r, z);
     st = check(cudaStreamEndCapture(stream_, &graph), "graph capture end");
     if (!st) return st;
     size_t nodes = 0;
     cudaGraphGetNodes(graph, nullptr, &nodes);
     mg_nodes_[slot] = nodes;
-    st = check(cudaGraphInstantiate(&mg_graph_[slot], graph, 0), "graph instantiate");
+    st = check(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
     cudaGraphDestroy(graph);
     if (!st) return st;
+    mg_graphs_.push_back(MgGraph{slot, r, z, exec});
   }
   launches_ += mg_nodes_[slot];
-  return check(cudaGraphLaunch(mg_graph_[slot], stream_), "graph launch");
+  return check(cudaGraphLaunch(exec, stream_), "graph launch");
 }
 
 Status Solver::dic_apply() {
@@ -1046,6 +1054,7 @@ Status Solver::ensure_fgmres_storage(uint32_t restart) {
   if (fg_storage_ != nullptr) {
     Status st = check(cudaStreamSynchronize(stream_), "fgmres storage");
     if (!st) return st;
+    clear_mg_graphs();  // graphs captured on the old basis buffers
     cudaFree(fg_storage_);
     fg_storage_ = nullptr;
   }
@@ -1410,15 +1419,22 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
     g[0] = beta;
     bool restarted = false;
     for (uint32_t column = 0; column < restart && it < control.maximum_iterations; ++column) {
-      // z_j = M v_j through the MG graph's fixed input/output buffers.
-      launch_copy(stream_, n, V[column], kr_);
-      launches_ += 1;
-      st = precondition(mixed);
-      if (!st) return st;
+      // z_j = M v_j: the MG graph of this column's buffers, or the cold
+      // path through the internal r/z buffers.
+      if (policy_.preconditioner != HFPS_PRECONDITIONER_IC0) {
+        st = mg_apply(mixed, V[column], Z[column]);
+        if (!st) return st;
+      } else {
+        launch_copy(stream_, n, V[column], kr_);
+        launches_ += 1;
+        st = precondition(mixed);
+        if (!st) return st;
+        launch_copy(stream_, n, kz_, Z[column]);
+        launches_ += 1;
+      }
       ++result.preconditioner_applies;
-      launch_copy(stream_, n, kz_, Z[column]);
       launch_operator_shift(stream_, A, Z[column], V[column], kShift, w);
-      launches_ += 2;
+      launches_ += 1;
       ++result.operator_applies;
       const int count = static_cast<int>(column) + 1;
       st = multidot(count, true);

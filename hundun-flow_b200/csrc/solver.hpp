@@ -96,8 +96,9 @@ class Solver {
   Status refresh_mixed();
   void aggregate_channel(int level, int face_axis, const double* src,
                          double* dst);
-  // The MG preconditioner: z = M r on the internal r/z buffers.
-  Status mg_apply(bool mixed);
+  // The MG preconditioner: z = M r, by default on the internal r/z buffers.
+  Status mg_apply(bool mixed, const double* r = nullptr, double* z = nullptr);
+  void clear_mg_graphs();
   // z = M r on kr_/kz_ with the policy's preconditioner (MG or cold IC(0)).
   Status precondition(bool mixed);
   Status dic_apply();
@@ -196,7 +197,16 @@ class Solver {
   double* dic_inv_{};
   cudaGraphExec_t dic_graph_{};
   size_t dic_nodes_{};
-  cudaGraphExec_t mg_graph_[2]{};
+  // The MG application captured as one CUDA graph per (precision slot,
+  // input, output) buffers: the PCG uses kr_/kz_, FGMRES every basis
+  // column's V_j/Z_j directly (no copies into fixed buffers).
+  struct MgGraph {
+    int slot;
+    const double* r;
+    double* z;
+    cudaGraphExec_t exec;
+  };
+  std::vector<MgGraph> mg_graphs_;
   size_t mg_nodes_[2]{};      // kernels per MG application (graph nodes)
   uint64_t launches_{};       // kernels launched since the last reset
   bool use_graphs_{true};
