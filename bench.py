@@ -50,8 +50,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--shape", type=int, nargs=3, default=None,
                    help="override the grid (testing only; the bench line is the 256^3 case)")
-    p.add_argument("--single", choices=["fp64", "mixed"], default=None,
-                   help="profiling aid: one warm-up solve, then one solve, no timing/JSON")
+    p.add_argument("--single", choices=["fp64", "mixed", "fgmres", "fgmres-mixed"], default=None,
+                   help="profiling aid: one warm-up solve, then one solve, no timing/JSON "
+                        "(PCG, or the production FGMRES(12) with the residual-minimising MG)")
     p.add_argument("--config", choices=["three_spheres512"], default=None,
                    help="the 512^3 three-sphere mixed forward + adjoint sequence "
                         "(its own JSON line; not the headline metric)")
@@ -471,14 +472,18 @@ def run_single(args):
     import hfps
     from hfps import workloads
     system = make_system(args)
-    solver = hfps.PressureSolver.from_system(system, hfps.Policy.production(),
-                                             stream=torch.cuda.current_stream())
+    fgmres = args.single.startswith("fgmres")
+    policy = hfps.Policy.production()
+    if fgmres:
+        policy = policy.replace(unit_linear=0)
+    solver = hfps.PressureSolver.from_system(system, policy, stream=torch.cuda.current_stream())
     rhs = torch.from_numpy(system.rhs.reshape(-1)).cuda()
     rhs1 = rhs + workloads.flux_divergence_rhs_torch(1, system.faces, system.boundary,
                                                      system.active, 0.05)
-    precision = hfps.MIXED if args.single == "mixed" else hfps.FP64
+    precision = hfps.MIXED if args.single.endswith("mixed") else hfps.FP64
+    extra = dict(algorithm=hfps.FGMRES, restart=12) if fgmres else {}
     opts = hfps.SolveOptions(rtol=RTOL, maxit=400, true_residual_interval=TRUE_RESIDUAL_INTERVAL,
-                             precision=precision)
+                             precision=precision, **extra)
     x, info0 = solver.solve(rhs, options=opts, history=False)
     x, info1 = solver.solve(rhs1, x0=x, out=x, options=opts, history=False)
     torch.cuda.synchronize()
