@@ -282,30 +282,6 @@ __global__ void __launch_bounds__(kRowThreads)
   cx[cc] = T(0);
 }
 
-template <class T>
-__global__ void k_restrict(Level<T> F, const T* __restrict__ r, Level<T> C,
-                           T* __restrict__ cb, T* __restrict__ cx, int mask) {
-  grid_dependency_sync();
-  const int n = C.nx * C.ny * C.nz;
-  const int mx = mask & 1, my = (mask >> 1) & 1, mz = (mask >> 2) & 1;
-  for (int cc = blockIdx.x * blockDim.x + threadIdx.x; cc < n;
-       cc += gridDim.x * blockDim.x) {
-    int ci, cj, ck;
-    cell_coords(cc, C.nx, C.ny, ci, cj, ck);
-    const int xb = mx ? 2 * ci : ci, yb = my ? 2 * cj : cj, zb = mz ? 2 * ck : ck;
-    T sum = T(0);
-    for (int dz = 0; dz <= mz; ++dz)
-      for (int dy = 0; dy <= my; ++dy)
-        for (int dx = 0; dx <= mx; ++dx) {
-          const int fi = xb + dx, fj = yb + dy, fk = zb + dz;
-          if (fi >= F.nx || fj >= F.ny || fk >= F.nz) continue;
-          sum += r[fi + F.nx * (fj + F.ny * fk)];
-        }
-    cb[cc] = sum;
-    cx[cc] = T(0);
-  }
-}
-
 // Trilinear prolongation and add, zero on solid cells (prolongate_cell).
 // One block per fine x-row (blockIdx.x; blockIdx.y splits long rows), one
 // vector entry per thread (natural order, or split rows walked entry by
@@ -1299,11 +1275,6 @@ void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
   }
 }
 template <class T>
-void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
-                     const Level<T>& C, T* cb, T* cx, int mask) {
-  launch(k_restrict<T>, grid_for(HFPS_CELLS(C)), kThreads, 0, s, F, r, C, cb, cx, mask);
-}
-template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int mask, int hx, int hxc) {
   int threads = 0;
@@ -1565,8 +1536,6 @@ void launch_adjoint_source(cudaStream_t s, int n, const double* dl_dp,
   template void launch_defect_restrict<T>(cudaStream_t, const Level<T>&, const T*, \
                                           const T*, const Level<T>&, T*, T*, int,  \
                                           int, int);                               \
-  template void launch_restrict<T>(cudaStream_t, const Level<T>&, const T*,        \
-                                   const Level<T>&, T*, T*, int);                  \
   template void launch_prolongate<T>(cudaStream_t, const Level<T>&, T*,            \
                                      const Level<T>&, const T*, int, int, int);    \
   template void launch_mg_enter<T>(cudaStream_t, int, const double*,               \

@@ -80,9 +80,6 @@ template <class T>
 void launch_defect_restrict(cudaStream_t s, const Level<T>& F, const T* x,
                             const T* b, const Level<T>& C, T* cb, T* cx,
                             int coarsen_mask, int hx = 0, int hxc = 0);
-template <class T>
-void launch_restrict(cudaStream_t s, const Level<T>& F, const T* r,
-                     const Level<T>& C, T* cb, T* cx, int coarsen_mask);
 // Fine x in layout hx, coarse x in layout hxc.
 template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,

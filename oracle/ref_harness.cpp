@@ -188,8 +188,8 @@ class HarnessOperator final : public LinearOperator {
 
 // Forwards to the MG plan but certifies it as the fixed SPD preconditioner
 // solve_pcg demands (src/solver_krylov.cpp:962-966).  The reference itself
-// has no MG-PCG route; this adapter is the one the north star's "MG-PCG"
-// parity comparison is defined against.
+// has no MG-PCG route; the MG-preconditioned CG solves of this library are
+// compared against this adapter.
 class PcgAdapter final : public LinearPreconditioner {
  public:
   NativeCartesianMgPlan* plan{};
