@@ -285,7 +285,7 @@ def run_reference(args, world, rank):
 # kernel (split-row vectors, a pass that reads x), from one ncu capture at
 # 256x256x128 (337.1 MB read + 26.1 MB written over 8,388,608 cells);
 # traffic grows with the cell count.
-LINE_PASS_DRAM_BYTES_PER_CELL = (337.118720e6 + 26.119936e6) / (256 * 256 * 128)
+LINE_PASS_DRAM_BYTES_PER_CELL = (303.605760e6 + 26.895872e6) / (256 * 256 * 128)
 
 # Iterations the reference solve_pcg (production MG, unit_linear) needs per
 # warm-started solve of this workload: 41, 41, 41 for steps 1-3, measured by

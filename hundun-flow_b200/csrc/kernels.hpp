@@ -93,9 +93,10 @@ void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
 constexpr long long kLinePcrThreshold = 1024;
 enum LineKind : int { kLineNone = 0, kLineScan = 1, kLinePcr = 2 };
 int line_kind(int nx, int ny, int nz, int axis);
-// Values of the factor block of one level and line axis: the Thomas
-// reciprocal, lower multiplier and upper multiplier (3 per cell), or PCR
-// multipliers and final diagonals.
+// Values of the factor block of one level and line axis in precision T: the
+// Thomas reciprocal and upper multiplier (2 per cell, FP64), plus the lower
+// multiplier (3 per cell, FP32), or PCR multipliers and final diagonals.
+template <class T>
 size_t line_factor_values(int nx, int ny, int nz, int axis);
 template <class T>
 void launch_line_factors(cudaStream_t s, const Level<T>& L, int axis, T* fac);

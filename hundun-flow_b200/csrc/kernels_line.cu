@@ -148,12 +148,18 @@ struct LineRhs {
 // Chunked-scan line solve.
 //
 // Each line's matrix is factorised once (full-line Thomas, in FP64): for row
-// s, den_s = b_s - a_s c'_{s-1}, and the sweep needs only
+// s, den_s = b_s - a_s c'_{s-1}, and the sweep needs
 //   inv_s = 1 / den_s,   l_s = a_s / den_s,   u_s = c'_s = c_s / den_s.
 // A sweep is then two first-order linear recurrences,
 //   forward   y_s = d_s inv_s - l_s y_{s-1},
-//   backward  x_s = y_s - u_s x_{s+1},
-// each an affine map per row.  A thread owns a chunk of up to
+//   backward  x_s = y_s - u_s x_{s+1}.
+// The line matrix is symmetric (a_s and c_{s-1} are the same face), so
+// a_s / den_{s-1} = u_{s-1}, and the LDL^T form of the forward recurrence
+//   z_s = d_s - u_{s-1} z_{s-1},   y_s = z_s inv_s
+// needs no l array.  FP64 sweeps use it (one stream of 8 B per row less);
+// FP32 sweeps keep the l array, because the extra load in the forward
+// replay costs the FP32 kernel registers and occupancy.
+// Each recurrence is an affine map per row.  A thread owns a chunk of up to
 // ScanConfig<T>::rows consecutive rows of one line: it composes its chunk's
 // maps, the chunks of a line combine their compositions through shared
 // memory, and every thread replays its chunk from the incoming value.  No spike vectors or interface
@@ -162,8 +168,8 @@ struct LineRhs {
 // stays in registers between the passes.
 //
 // Factor layout is colour-packed so that threads with consecutive line
-// indices of one colour read consecutive addresses: array e (0 inv, 1 l,
-// 2 u) of row s of colour line t sits at
+// indices of one colour read consecutive addresses: array e (0 inv, then
+// 1 u in the symmetric form, or 1 l and 2 u) of row s of colour line t sits at
 //   ((e * 2 + colour) * extent + s) * colour_lines + t.
 
 // Rows per chunk (held in registers) and the block-size bound, per
@@ -189,11 +195,15 @@ template <>
 struct ScanConfig<double> {
   static constexpr int rows = HFPS_SCAN_ROWS_F64;
   static constexpr int threads = HFPS_SCAN_THREADS_F64;
+  static constexpr bool symmetric = true;
+  static constexpr int arrays = 2;
 };
 template <>
 struct ScanConfig<float> {
   static constexpr int rows = HFPS_SCAN_ROWS_F32;
   static constexpr int threads = HFPS_SCAN_THREADS_F32;
+  static constexpr bool symmetric = false;
+  static constexpr int arrays = 3;
 };
 // Longest line both precisions can solve: every chunk of a line lives in
 // one block.
@@ -201,7 +211,6 @@ constexpr int kScanMaxExtent =
     HFPS_SCAN_ROWS_F64 * HFPS_SCAN_THREADS_F64 < HFPS_SCAN_ROWS_F32 * HFPS_SCAN_THREADS_F32
         ? HFPS_SCAN_ROWS_F64 * HFPS_SCAN_THREADS_F64
         : HFPS_SCAN_ROWS_F32 * HFPS_SCAN_THREADS_F32;
-constexpr int kScanArrays = 3;
 
 struct ScanLayout {
   int extent;
@@ -209,8 +218,8 @@ struct ScanLayout {
   __host__ __device__ size_t cell(int e, int colour, int s, int t) const {
     return ((static_cast<size_t>(e) * 2 + colour) * extent + s) * colour_lines + t;
   }
-  __host__ __device__ size_t values() const {
-    return static_cast<size_t>(kScanArrays) * 2 * extent * colour_lines;
+  __host__ __device__ size_t values(int arrays) const {
+    return static_cast<size_t>(arrays) * 2 * extent * colour_lines;
   }
 };
 
@@ -244,8 +253,12 @@ __global__ void k_scan_factors(Level<T> L, int axis, T* __restrict__ fac) {
       const double den = static_cast<double>(L.diag[c]) - a * prev_u;
       const double u = cc / den;
       fac[lay.cell(0, colour, s, t)] = static_cast<T>(1.0 / den);
-      fac[lay.cell(1, colour, s, t)] = static_cast<T>(a / den);
-      fac[lay.cell(2, colour, s, t)] = static_cast<T>(u);
+      if constexpr (ScanConfig<T>::symmetric) {
+        fac[lay.cell(1, colour, s, t)] = static_cast<T>(u);
+      } else {
+        fac[lay.cell(1, colour, s, t)] = static_cast<T>(a / den);
+        fac[lay.cell(2, colour, s, t)] = static_cast<T>(u);
+      }
       prev_u = u;
     }
   }
@@ -291,26 +304,39 @@ __global__ void __launch_bounds__(ScanConfig<T>::threads)
   const int rows = valid ? max(0, min(m, extent - r0)) : 0;
   const int row = lay.colour_lines;
   const int tt = valid ? t : 0;
+  constexpr bool kSym = ScanConfig<T>::symmetric;
   const T* inv = fac + lay.cell(0, color, 0, tt);
   const T* lf = fac + lay.cell(1, color, 0, tt);
-  const T* uf = fac + lay.cell(2, color, 0, tt);
+  const T* uf = fac + lay.cell(kSym ? 1 : 2, color, 0, tt);
   // Rows past the chunk's end (padding, and every row of an idle thread)
   // re-read the line's last row so that all loads are unconditional; their
   // values are never used.
   const auto srow = [&](int u) { return min(r0 + u, extent - 1); };
+  // Forward multiplier of row s: u_{s-1} (zero on row 0), or l_s.
+  const auto lower = [&](int u) -> T {
+    const int s = srow(u);
+    if constexpr (kSym) {
+      const T g = __ldg(uf + max(s - 1, 0) * row);
+      return s > 0 ? g : T(0);
+    } else {
+      return __ldg(lf + s * row);
+    }
+  };
 
-  // Pass 1: right-hand sides scaled by 1/den, and the forward composition.
+  // Pass 1: right-hand sides (scaled by 1/den unless symmetric), and the
+  // forward composition.
   const LineRhs<T, AXIS, SPLIT> lr(L, valid ? fa : 0, valid ? fb : 0, hx);
   constexpr int kScanRows = ScanConfig<T>::rows;
   T v[kScanRows];
 #pragma unroll
-  for (int u = 0; u < kScanRows; ++u)
-    v[u] = lr.template row<MODE>(x, rhs, base + srow(u) * stride, srow(u), extent) *
-           __ldg(inv + srow(u) * row);
+  for (int u = 0; u < kScanRows; ++u) {
+    v[u] = lr.template row<MODE>(x, rhs, base + srow(u) * stride, srow(u), extent);
+    if constexpr (!kSym) v[u] = v[u] * __ldg(inv + srow(u) * row);
+  }
   T A = T(1), B = T(0);
 #pragma unroll
   for (int u = 0; u < kScanRows; ++u) {
-    const T l = __ldg(lf + srow(u) * row);
+    const T l = lower(u);
     const bool on = u < rows;
     B = on ? v[u] - l * B : B;
     A = on ? -l * A : A;
@@ -318,13 +344,17 @@ __global__ void __launch_bounds__(ScanConfig<T>::threads)
   fA[q * LPB + lane] = A;
   fB[q * LPB + lane] = B;
   __syncthreads();
-  // Forward replay from y_{r0-1}.
-  T y = T(0);
-  for (int p = 0; p < q; ++p) y = fA[p * LPB + lane] * y + fB[p * LPB + lane];
+  // Forward replay from z_{r0-1} (y_{r0-1}); v becomes y.
+  T z = T(0);
+  for (int p = 0; p < q; ++p) z = fA[p * LPB + lane] * z + fB[p * LPB + lane];
 #pragma unroll
   for (int u = 0; u < kScanRows; ++u) {
-    y = v[u] - __ldg(lf + srow(u) * row) * y;
-    v[u] = y;
+    z = v[u] - lower(u) * z;
+    if constexpr (kSym) {
+      v[u] = z * __ldg(inv + srow(u) * row);
+    } else {
+      v[u] = z;
+    }
   }
   // Backward composition x_{r0} = A x_{r1+1} + B.
   A = T(1);
@@ -628,6 +658,7 @@ int line_kind(int nx, int ny, int nz, int axis) {
   return extent <= kScanMaxExtent ? kLineScan : kLineNone;
 }
 
+template <class T>
 size_t line_factor_values(int nx, int ny, int nz, int axis) {
   const int extent = line_extent(axis, nx, ny, nz);
   const int a_extent = axis == 0 ? ny : nx;
@@ -635,7 +666,8 @@ size_t line_factor_values(int nx, int ny, int nz, int axis) {
   const size_t lines = static_cast<size_t>(a_extent) * b_extent;
   const int kind = line_kind(nx, ny, nz, axis);
   if (kind == kLineNone) return 0;
-  if (kind == kLineScan) return ScanLayout{extent, ((a_extent + 1) / 2) * b_extent}.values();
+  if (kind == kLineScan)
+    return ScanLayout{extent, ((a_extent + 1) / 2) * b_extent}.values(ScanConfig<T>::arrays);
   int P, lpb, steps;
   pcr_shape(extent, P, lpb, steps);
   return static_cast<size_t>(2 * steps + 1) * lines * P;
@@ -731,6 +763,8 @@ bool launch_coarse_line(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
   return true;
 }
 
+template size_t line_factor_values<double>(int, int, int, int);
+template size_t line_factor_values<float>(int, int, int, int);
 template void launch_line_factors<double>(cudaStream_t, const Level<double>&, int, double*);
 template void launch_line_factors<float>(cudaStream_t, const Level<float>&, int, float*);
 template void launch_line_pass<double>(cudaStream_t, const Level<double>&, double*,

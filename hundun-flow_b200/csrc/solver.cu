@@ -266,9 +266,8 @@ Status Solver::allocate() {
     for (int a = 0; a < 3; ++a) {
       o.lf64[a] = o.lf32[a] = SIZE_MAX;
       if (!(s.line_mask & (1 << a))) continue;
-      const size_t values = line_factor_values(s.n[0], s.n[1], s.n[2], a);
-      o.lf64[a] = add(values * 8);
-      o.lf32[a] = add(values * 4);
+      o.lf64[a] = add(line_factor_values<double>(s.n[0], s.n[1], s.n[2], a) * 8);
+      o.lf32[a] = add(line_factor_values<float>(s.n[0], s.n[1], s.n[2], a) * 4);
     }
   }
   const size_t cells = static_cast<size_t>(nx_) * ny_ * nz_;
