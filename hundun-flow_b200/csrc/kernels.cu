@@ -309,6 +309,75 @@ __global__ void __launch_bounds__(kRowThreads)
                          F, x, C, cx, MASK, c, i, j, k, at, SplitPos{C.ny, hxc});
 }
 
+// Prolongation for x/z coarsening (mask 5, y kept: the levels of y-line
+// relaxation) into split fine rows.  A thread takes the up to 2x2 fine cells
+// (2p + dx, j, 2q + dz) over coarse cell (p, j, q).  Their stencils lie in
+// coarse cells p-1..p+1 x q-1..q+1, so the nine values are loaded once
+// (indices clamped into the level).  Fine cell dx takes its left and right
+// x-candidates from columns dx and dx+1 of that block (rows dz and dz+1 in
+// z): interp_axis's candidates are p-1/p (even) and p/p+1 (odd), and where it
+// clamps at a level edge the clamped load holds the same cell.  Each fine
+// value is then formed exactly as prolongate_cell forms it (same weights,
+// terms and order), so results are bit-identical to k_prolongate<T, 5>.
+template <class T, class CPos>
+__global__ void __launch_bounds__(kRowThreads)
+    k_prolongate_xz(Level<T> F, T* __restrict__ x, Level<T> C, const T* __restrict__ cx,
+                    int hx, CPos cpos) {
+  grid_dependency_sync();
+  const int crow = blockIdx.x;  // j + ny * q (the coarse level keeps ny)
+  const int p = blockIdx.y * blockDim.x + threadIdx.x;
+  if (p >= C.nx) return;
+  const int q = crow / F.ny;
+  const int j = crow - q * F.ny;
+  T v[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int zq = min(max(q + a - 1, 0), C.nz - 1);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const int xp = min(max(p + b - 1, 0), C.nx - 1);
+      v[a][b] = __ldg(cx + cpos(xp + C.nx * (j + C.ny * zq), xp, j, zq));
+    }
+  }
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz) {
+    const int k = 2 * q + dz;
+    if (k >= F.nz) break;
+    int zl, zr;
+    double zw;
+    interp_axis(k, 1, C.nz, zl, zr, zw);
+    const bool two_z = zl != zr;
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx) {
+      const int i = 2 * p + dx;
+      if (i >= F.nx) break;
+      int xl, xr;
+      double xw;
+      interp_axis(i, 1, C.nx, xl, xr, xw);
+      const bool two_x = xl != xr;
+      const int c = i + F.nx * (j + F.ny * k);
+      const int at = 2 * hx * (j + F.ny * k) + dx * hx + p;
+      const bool fluid = F.fluid[c] != 0;
+      const T old = x[at];
+      T value = T(0);
+#pragma unroll
+      for (int az = 0; az < 2; ++az)
+#pragma unroll
+        for (int ax = 0; ax < 2; ++ax) {
+          const double wz = az == 0 ? 1.0 - zw : zw;
+          const double wy = 1.0;
+          const double wx = ax == 0 ? 1.0 - xw : xw;
+          const T w = static_cast<T>(wx * wy * wz);
+          const T term = w * v[dz + az][dx + ax];
+          const bool on = (az == 0 || two_z) && (ax == 0 || two_x);
+          const T sum = value + term;
+          value = on ? sum : value;
+        }
+      x[at] = fluid ? old + value : T(0);
+    }
+  }
+}
+
 // Coarsest level: `sweeps` smoother sweeps in one CTA (mg_cycle coarse
 // branch, src/solver_mg.cpp:4210-4227).  The state is widened to TC (FP64
 // in the mixed-precision hierarchy) for the duration of the solve.
@@ -1278,6 +1347,15 @@ template <class T>
 void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int mask, int hx, int hxc) {
   int threads = 0;
+  if ((mask & 7) == 5 && hx != 0) {
+    const dim3 grid = row_grid(F.ny * C.nz, C.nx, threads);
+    if (hxc != 0)
+      launch(k_prolongate_xz<T, SplitPos>, grid, threads, 0, s, F, x, C, cx, hx,
+             SplitPos{C.ny, hxc});
+    else
+      launch(k_prolongate_xz<T, NaturalPos>, grid, threads, 0, s, F, x, C, cx, hx, NaturalPos());
+    return;
+  }
   const dim3 grid = row_grid(F.ny * F.nz, hx == 0 ? F.nx : 2 * hx, threads);
   switch (mask & 7) {
 #define HFPS_PROLONG_CASE(M)                                                              \
