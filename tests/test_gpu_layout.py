@@ -7,7 +7,8 @@ the MG entry clearing it; HFPS_SPLIT_ROWS=0 (read when the solver is created)
 keeps the natural order everywhere.  Both perform the same operations on the
 same values, so the MG application and whole solves must agree bit for bit:
 FP64 and mixed, unit and residual-minimising corrections, even and odd nx
-(the odd half of a split row then has a padding slot), y- and z-lines.
+(the odd half of a split row then has a padding slot), y- and z-lines, one
+and two split levels.
 """
 import os
 
@@ -43,6 +44,9 @@ def z_stretched(n):
 CASES = {
     "y_lines": lambda: workloads.make("wrinkled256", n=(96, 128, 64)),
     "y_lines_odd_nx": lambda: workloads.make("wrinkled256", n=(73, 150, 40)),
+    # levels 0 and 1 both in split rows, odd nx and nz on level 0 and odd nz on
+    # level 1: the 2x2 prolongation between split levels and at odd row ends
+    "y_lines_two_split_levels": lambda: workloads.make("wrinkled256", n=(131, 160, 133)),
     "z_lines": lambda: z_stretched((64, 48, 96)),
 }
 
