@@ -15,6 +15,10 @@ struct hfps_solver {
 
 namespace {
 
+// Reason for the calling thread's last failed hfps_create (no handle exists
+// to hold it); hfps_last_error(NULL) returns it.
+thread_local std::string create_error;
+
 int finish(hfps_solver* s, hfps::Status st) {
   if (!st && s != nullptr && s->impl != nullptr) s->error = s->impl->last_error();
   return st.code;
@@ -80,29 +84,38 @@ void hfps_default_control(hfps_control* c) {
 
 int hfps_create(const hfps_geometry* geometry, const hfps_policy* policy,
                 void* stream, hfps_solver** out) {
-  if (out == nullptr) return HFPS_INVALID_PLAN;
+  create_error.clear();
+  if (out == nullptr || geometry == nullptr) {
+    create_error = "null geometry or output handle";
+    return HFPS_INVALID_PLAN;
+  }
   *out = nullptr;
-  if (geometry == nullptr) return HFPS_INVALID_PLAN;
   hfps_policy defaults;
   hfps_default_policy(&defaults);
   try {
-    hfps_solver* handle = new hfps_solver();
     std::string error;
     hfps::Solver* impl = nullptr;
     const hfps::Status st = hfps::Solver::create(
         *geometry, policy != nullptr ? *policy : defaults,
         static_cast<cudaStream_t>(stream), &impl, error);
     if (!st) {
-      handle->error = error;
-      delete handle;
+      create_error = error;
       return st.code;
+    }
+    hfps_solver* handle = new (std::nothrow) hfps_solver();
+    if (handle == nullptr) {
+      delete impl;
+      create_error = "host allocation failure";
+      return HFPS_ALLOCATION_FAILURE;
     }
     handle->impl = impl;
     *out = handle;
     return HFPS_OK;
   } catch (const std::bad_alloc&) {
+    create_error = "host allocation failure";
     return HFPS_ALLOCATION_FAILURE;
   } catch (...) {
+    create_error = "unexpected host exception";
     return HFPS_INVALID_PLAN;
   }
 }
@@ -198,7 +211,7 @@ int hfps_profile_kernel(hfps_solver* s, int kernel, int repetitions,
 }
 
 const char* hfps_last_error(hfps_solver* s) {
-  if (s == nullptr) return "null solver handle";
+  if (s == nullptr) return create_error.empty() ? "null solver handle" : create_error.c_str();
   return s->error.c_str();
 }
 

@@ -262,7 +262,8 @@ class PressureSolver:
         rc = lib.hfps_create(ctypes.byref(g), ctypes.byref(self.policy), stream_ptr,
                              ctypes.byref(handle))
         if rc != 0:
-            raise SolverError(rc, "hfps_create failed")
+            msg = lib.hfps_last_error(None)
+            raise SolverError(rc, f"hfps_create: {msg.decode() if msg else ''}")
         self._handle = handle
         self._lib = lib
 

@@ -361,7 +361,8 @@ HFPS_API int hfps_operator_dot_noalloc(const hfps_operator_view* op,
                                        const double* x, double* y,
                                        double* x_dot_y, void* stream);
 
-/* Sticky error text of the last failing call on this handle. */
+/* Sticky error text of the last failing call on this handle.  With a NULL
+ * handle: the reason the calling thread's last hfps_create failed. */
 HFPS_API const char* hfps_last_error(hfps_solver* solver);
 
 HFPS_API int hfps_destroy(hfps_solver* solver);

@@ -45,11 +45,11 @@ def test_invalid_plans_are_rejected_before_any_device_work(cuda_library):
     import numpy as np
     from hfps import Policy, PressureSolver, SolverError
     faces = [np.linspace(0, 1, 5)] * 3
-    with pytest.raises(SolverError):
-        PressureSolver((4, 4, 4), faces, (2, 2, 0, 0, 0, 0))  # periodic unsupported
-    with pytest.raises(SolverError):
+    with pytest.raises(SolverError, match="periodic boundaries are not supported"):
+        PressureSolver((4, 4, 4), faces, (2, 2, 0, 0, 0, 0))
+    with pytest.raises(SolverError, match="invalid geometry or policy"):
         PressureSolver((4, 4, 4), faces, (0,) * 6, policy=Policy.default().replace(pre_sweeps=0))
-    with pytest.raises(SolverError):
+    with pytest.raises(SolverError, match="face coordinates must increase"):
         bad = [np.array([0, 0.5, 0.4, 0.8, 1.0])] * 3
         PressureSolver((4, 4, 4), bad, (0,) * 6)
 
