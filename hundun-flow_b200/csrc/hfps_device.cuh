@@ -23,8 +23,9 @@
 // preceding grid has completed and its writes are visible, before touching
 // any memory.  Kernels launched without the attribute pass it straight
 // through.  An early launch_dependents trigger (dependents scheduled while
-// this grid still runs) measured 3% faster on the FP64 MG cycle but 7%
-// slower on the FP32 one at 256^3, so dependents launch at grid exit.
+// this grid still runs) measured slower at 256^3: 7% on the FP32 MG cycle,
+// and 3% on the FP64 one when given to the FP64 kernels alone (2.79 -> 2.88
+// ms), so dependents launch at grid exit.
 #ifndef HFPS_USE_PDL
 #define HFPS_USE_PDL 1
 #endif
