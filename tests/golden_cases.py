@@ -44,3 +44,34 @@ def digest(s):
     if s.active is not None:
         h.update(np.ascontiguousarray(s.active, dtype=np.uint8).tobytes())
     return h.hexdigest()
+
+
+def anisotropic_x_system():
+    """The line-relaxation fixture of tests/numerical/
+    solver_mg_line_relaxation_test.cpp:33-44, 236-265: 64x12x8 uniform cells
+    on [0, 0.05] x [0, 1] x [0, 1] (x strongly coupled), constant face
+    coefficients 1/h^2 on every face, diagonal 2 (ax + ay + az), Dirichlet
+    on all six sides, rhs the product of half-period sines."""
+    from hfps import workloads
+    nx, ny, nz = 64, 12, 8
+    faces = (np.linspace(0.0, 0.05, nx + 1), np.linspace(0.0, 1.0, ny + 1),
+             np.linspace(0.0, 1.0, nz + 1))
+    ax, ay, az = (1.0 / (np.diff(f)[0] ** 2) for f in faces)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    rhs = (np.sin(np.pi * (i + 0.5) / nx) * np.sin(np.pi * (j + 0.5) / ny)
+           * np.sin(np.pi * (k + 0.5) / nz))
+    return workloads.PressureSystem(
+        "anisotropic_x", (nx, ny, nz), faces, (workloads.DIRICHLET,) * 6,
+        np.ones((nz, ny, nx)), np.full((nz, ny, nx), 2.0 * (ax + ay + az)),
+        np.full((nz, ny, nx + 1), ax), np.full((nz, ny + 1, nx), ay),
+        np.full((nz + 1, ny, nx), az), None, np.ascontiguousarray(rhs))
+
+
+def line_relaxation_policy(lines=True):
+    """That test's MG spec: Chebyshev-Jacobi V(1,1), 16 coarse sweeps, at
+    most 12 levels, anisotropy threshold 4.  Without lines the threshold is
+    raised past any anisotropy, which also gives up semicoarsening (the
+    reference test keeps the coarsening and clears only the line axes)."""
+    import ref_oracle
+    return ref_oracle.MgPolicy(smoother=1, cycle=0, pre=1, post=1, coarse_sweeps=16,
+                               max_levels=12, anisotropy_threshold=4.0 if lines else 1e300)

@@ -105,6 +105,32 @@ def test_mg_scan_lines_match(hfps_mod, shape):
     assert rel(g.apply_preconditioner(v), o.apply_mg(v)) <= 1e-13
 
 
+def test_line_relaxation_outperforms_point_smoothing(hfps_mod):
+    """The reference's line-relaxation fixture (tests/numerical/
+    solver_mg_line_relaxation_test.cpp:316-335) on the GPU: x-lines (PCR
+    colour passes) match the restatement's zebra cycle to line-mode rounding,
+    point-only smoothing matches it bit for bit, and the line cycle keeps the
+    reference test's bounds (<= 0.10 of the initial residual, <= 0.70 of the
+    point-only residual)."""
+    s = golden_cases.anisotropic_x_system()
+    residual = {}
+    for lines in (True, False):
+        pol = golden_cases.line_relaxation_policy(lines)
+        g = hfps_mod.PressureSolver.from_system(s, gpu_policy(hfps_mod, pol))
+        o = oracle(s, pol, line_order=1)
+        assert g.levels()[0][3] == (1 if lines else 0)
+        z = g.apply_preconditioner(s.rhs)
+        zo = o.apply_mg(s.rhs)
+        if lines:
+            assert rel(z, zo) <= 1e-11
+        else:
+            assert np.array_equal(z, zo)
+        residual[lines] = np.linalg.norm(s.rhs - o.apply_operator(z))
+        g.close()
+    assert residual[True] <= 0.10 * np.linalg.norm(s.rhs)
+    assert residual[True] <= 0.70 * residual[False]
+
+
 def stretched_front(n, axis, ratio=1.05):
     """A wrinkled density front on a grid stretched along `axis` (0 x, 2 z)."""
     faces = [workloads.uniform_faces(m) for m in n]

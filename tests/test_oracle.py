@@ -10,8 +10,10 @@ The C restatement (oracle/hfps_oracle.c) is pinned three ways:
   Chebyshev degrees 1-4 (tests/unit/solver_mg_chebyshev_test.cpp:797-841),
   IBM operator equivalence (tests/unit/solver_ibm_pressure_operator_test.cpp:
   131-233), monotone MG contraction (tests/numerical/
-  solver_mg_convergence_test.cpp:630-800) and PCG against an independent
-  direct solve (tests/mpi/solver_krylov_mpi_test.cpp:1141-1193).
+  solver_mg_convergence_test.cpp:630-800), line relaxation against point
+  smoothing (tests/numerical/solver_mg_line_relaxation_test.cpp:316-335) and
+  PCG against an independent direct solve (tests/mpi/
+  solver_krylov_mpi_test.cpp:1141-1193).
 """
 import dataclasses
 import os
@@ -233,6 +235,25 @@ def test_mg_cycles_contract_monotonically():
         norms.append(np.linalg.norm(r))
     assert all(b <= a * (1 + 1e-12) for a, b in zip(norms, norms[1:]))
     assert norms[-1] <= 0.5 * norms[0]
+
+
+@pytest.mark.parametrize("line_order", [0, 1])
+def test_line_relaxation_outperforms_point_smoothing(line_order):
+    """One MG application from zero on the strongly x-coupled 64x12x8 mesh
+    (tests/numerical/solver_mg_line_relaxation_test.cpp:316-335): x-lines are
+    selected, the cycle leaves at most 0.10 of the initial residual, and at
+    most 0.70 of what point-only smoothing leaves.  Lexicographic (the
+    reference's) and zebra (the CUDA path's) line orders."""
+    s = golden_cases.anisotropic_x_system()
+    residual = {}
+    for lines in (True, False):
+        o = _oracle(s, golden_cases.line_relaxation_policy(lines), line_order=line_order)
+        assert o.levels()[0][3] == (1 if lines else 0)
+        z = o.apply_mg(s.rhs)
+        assert np.all(np.isfinite(z))
+        residual[lines] = np.linalg.norm(s.rhs - o.apply_operator(z))
+    assert residual[True] <= 0.10 * np.linalg.norm(s.rhs)
+    assert residual[True] <= 0.70 * residual[False]
 
 
 def test_pcg_matches_direct_solve():
