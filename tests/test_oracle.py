@@ -10,7 +10,8 @@ The C restatement (oracle/hfps_oracle.c) is pinned three ways:
   Chebyshev degrees 1-4 (tests/unit/solver_mg_chebyshev_test.cpp:797-841),
   IBM operator equivalence (tests/unit/solver_ibm_pressure_operator_test.cpp:
   131-233), monotone MG contraction (tests/numerical/
-  solver_mg_convergence_test.cpp:630-800), line relaxation against point
+  solver_mg_convergence_test.cpp:630-800), the diagonal shortcut
+  (tests/unit/solver_mg_chebyshev_test.cpp:1250-1300), line relaxation against point
   smoothing (tests/numerical/solver_mg_line_relaxation_test.cpp:316-335) and
   PCG against an independent direct solve (tests/mpi/
   solver_krylov_mpi_test.cpp:1141-1193).
@@ -165,6 +166,33 @@ def _uniform_system(n, diag, face, boundary=(0, 0, 0, 0, 0, 0), active=None, rhs
         rhs = np.zeros((nz, ny, nx))
     return workloads.PressureSystem("uniform", (nx, ny, nz), faces, tuple(boundary),
                                     np.ones((nz, ny, nx)), d, fx, fy, fz, active, rhs)
+
+
+def test_diagonal_shortcut_known_answer():
+    """Strong diagonal dominance takes the masked diagonal inverse instead of
+    a cycle (tests/unit/solver_mg_chebyshev_test.cpp:1250-1300): on 8^3 cells
+    with diagonal 100, unit faces and a solid corner cell, the correction is
+    r / 100, r / 99 on the three cells that lost a face to the solid, 0 on the
+    solid; a weakly dominant diagonal (7) runs the cycle again.  The
+    restatement and, when built, the compiled reference."""
+    import ref_oracle
+    rng = np.random.default_rng(17)
+    active = np.ones((8, 8, 8), np.uint8)
+    active[0, 0, 0] = 0
+    pol = ref_oracle.MgPolicy(smoother=1, cycle=0, pre=2, post=2, diagonal_shortcut=0.1)
+    k, j, i = np.meshgrid(np.arange(8), np.arange(8), np.arange(8), indexing="ij")
+    expected_divisor = np.where(i + j + k == 1, 99.0, 100.0)
+    r = rng.standard_normal((8, 8, 8)) * active
+    sessions = [lambda s: _oracle(s, pol)]
+    if ref_oracle.available():
+        sessions.append(lambda s: ref_oracle.RefSession(s, pol, algorithm="pcg"))
+    for make in sessions:
+        strong = make(_uniform_system((8, 8, 8), 100.0, 1.0, active=active))
+        z = strong.apply_mg(r)
+        assert np.array_equal(z, np.where(active == 1, r / expected_divisor, 0.0))
+        weak = make(_uniform_system((8, 8, 8), 7.0, 1.0, active=active))
+        zw = weak.apply_mg(r)
+        assert np.all(np.isfinite(zw)) and not np.allclose(zw, r / 7.0)
 
 
 def _scalar_chebyshev(rhs, diagonal, eigenvalue, stages, fraction):
