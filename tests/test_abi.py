@@ -52,6 +52,12 @@ def test_invalid_plans_are_rejected_before_any_device_work(cuda_library):
     with pytest.raises(SolverError, match="face coordinates must increase"):
         bad = [np.array([0, 0.5, 0.4, 0.8, 1.0])] * 3
         PressureSolver((4, 4, 4), bad, (0,) * 6)
+    # the Chebyshev lower-spectrum fraction must lie strictly inside (0, 1)
+    # (tests/unit/solver_mg_chebyshev_test.cpp:1237-1243)
+    for fraction in (0.0, 1.0, float("nan")):
+        with pytest.raises(SolverError, match="invalid geometry or policy"):
+            PressureSolver((4, 4, 4), faces, (0,) * 6, policy=Policy.production().replace(
+                chebyshev_lower_spectrum_fraction=fraction))
 
 
 def test_missing_gpu_fails_loudly(cuda_library):
