@@ -58,6 +58,12 @@ def test_invalid_plans_are_rejected_before_any_device_work(cuda_library):
         with pytest.raises(SolverError, match="invalid geometry or policy"):
             PressureSolver((4, 4, 4), faces, (0,) * 6, policy=Policy.production().replace(
                 chebyshev_lower_spectrum_fraction=fraction))
+    # and the diagonal-shortcut ratio inside [0, 1)
+    # (tests/unit/solver_mg_chebyshev_test.cpp:1307-1312)
+    for ratio in (-0.1, 1.0, float("nan")):
+        with pytest.raises(SolverError, match="invalid geometry or policy"):
+            PressureSolver((4, 4, 4), faces, (0,) * 6, policy=Policy.production().replace(
+                diagonal_shortcut_maximum_ratio=ratio))
 
 
 def test_missing_gpu_fails_loudly(cuda_library):

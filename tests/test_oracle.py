@@ -195,6 +195,23 @@ def test_diagonal_shortcut_known_answer():
         assert np.all(np.isfinite(zw)) and not np.allclose(zw, r / 7.0)
 
 
+def test_mg_correction_scales_with_the_residual():
+    """The MG correction of 1e-12 r is 1e-12 times that of r to 1e-12
+    relative (tests/unit/solver_mg_chebyshev_test.cpp:1358-1383: Chebyshev,
+    diagonal 7, unit faces, r = 1), for both correction scalings."""
+    import ref_oracle
+    pol = ref_oracle.MgPolicy(smoother=1, cycle=0, pre=2, post=2)
+    s = _uniform_system((8, 8, 8), 7.0, 1.0)
+    r = np.ones((8, 8, 8))
+    for unit_linear in (True, False):
+        o = _oracle(s, pol, unit_linear=unit_linear)
+        z = o.apply_mg(r)
+        zs = o.apply_mg(1e-12 * r)
+        magnitude = np.max(np.abs(z))
+        assert magnitude > 0.0
+        assert np.max(np.abs(zs / 1e-12 - z)) < 1e-12 * magnitude
+
+
 def _scalar_chebyshev(rhs, diagonal, eigenvalue, stages, fraction):
     beta = 2.0
     alpha = fraction * beta
