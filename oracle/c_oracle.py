@@ -157,9 +157,13 @@ class OracleSession:
               recycle: str = "none"):
         """solve_pcg, or solve_fgmres(restart) when ``algorithm == "fgmres"``
         (build the session with unit_linear=False for the reference's
-        residual-minimising MG scaling).  ``recycle`` as RefSession.solve."""
+        residual-minimising MG scaling).  ``recycle`` as RefSession.solve.
+        A solve that does not return ok publishes nothing: the returned x is
+        the initial guess, as the reference leaves the caller's solution
+        untouched for an unpublished candidate."""
         rhs = np.ascontiguousarray(rhs, dtype=np.float64)
         x = np.zeros_like(rhs) if x0 is None else np.array(x0, dtype=np.float64, order="C")
+        initial = x.copy()
         out = np.zeros(13)
         hist = np.zeros(maxit)
         if algorithm == "bicgstab":
@@ -191,4 +195,6 @@ class OracleSession:
             "recycle_projected_residual": out[11],
             "recycle_cycle_corrections": int(out[12]),
         }
+        if rc != 0:
+            x = initial
         return x, info

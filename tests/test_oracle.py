@@ -212,6 +212,26 @@ def test_mg_correction_scales_with_the_residual():
         assert np.max(np.abs(zs / 1e-12 - z)) < 1e-12 * magnitude
 
 
+@pytest.mark.parametrize("algorithm", ["pcg", "fgmres", "bicgstab"])
+def test_iteration_cap_publishes_nothing(algorithm):
+    """An iteration cap cannot masquerade as convergence
+    (tests/mpi/solver_krylov_mpi_test.cpp:1474-1487): one iteration allowed,
+    status rejected_step, termination maximum_iterations, and the caller's
+    solution untouched; the compiled reference (PCG, FGMRES) does the same."""
+    import ref_oracle
+    s = workloads.make("sphere64", n=(12, 10, 9), spheres=((0.5, 0.5, 0.5, 0.2),), seed=2)
+    x0 = 0.1 * np.ones_like(s.rhs)
+    o = _oracle(s, ref_oracle.MgPolicy(), unit_linear=algorithm != "fgmres")
+    x, info = o.solve(s.rhs, x0=x0, rtol=1e-12, maxit=1, algorithm=algorithm)
+    assert info["status"] == 6 and info["termination"] == "maximum_iterations"
+    assert info["iterations"] == 1 and np.array_equal(x, x0)
+    if ref_oracle.available() and algorithm != "bicgstab":
+        xr, ir = ref_oracle.RefSession(s, ref_oracle.MgPolicy(), algorithm=algorithm).solve(
+            s.rhs, x0=x0, rtol=1e-12, maxit=1)
+        assert ir["termination"] == "maximum_iterations" and ir["iterations"] == 1
+        assert np.array_equal(xr, x0)
+
+
 def _scalar_chebyshev(rhs, diagonal, eigenvalue, stages, fraction):
     beta = 2.0
     alpha = fraction * beta
