@@ -60,3 +60,32 @@ def test_assembly_diagonal_is_storage_plus_faces():
                        rtol=1e-12)
     # a0 + a1 + a2 = 0 with equal densities: only the flux divergence remains.
     assert np.allclose(rhs, -pressure_steps.outward_flux(*q), atol=1e-12)
+
+
+def test_boundary_jumps_and_flux_response_known_answers():
+    """The reference's boundary semantics for the correction jump and the
+    mass-flux response (tests/unit/solver_pressure_boundary_plan_test.cpp:
+    203-223): a Neumann face has zero jump, a Dirichlet face on the high side
+    has jump -p_owner (on the low side +p_owner: the boundary value is 0),
+    interior faces p_hi - p_lo, and the response with coefficient 3 is
+    -3 times the jump."""
+    import pressure_steps
+    N, D = pressure_steps.NEUMANN, workloads.DIRICHLET
+    rng = np.random.default_rng(9)
+    p = rng.standard_normal((3, 4, 5))  # (nz, ny, nx)
+    boundary = (N, D, D, N, N, D)
+    jx = pressure_steps._jump(p, 0, boundary)
+    jy = pressure_steps._jump(p, 1, boundary)
+    jz = pressure_steps._jump(p, 2, boundary)
+    assert np.array_equal(jx[:, :, 0], np.zeros((3, 4)))           # x-min Neumann
+    assert np.array_equal(jx[:, :, -1], -p[:, :, -1])               # x-max Dirichlet
+    assert np.array_equal(jx[:, :, 1:-1], p[:, :, 1:] - p[:, :, :-1])
+    assert np.array_equal(jy[:, 0, :], p[:, 0, :])                  # y-min Dirichlet
+    assert np.array_equal(jy[:, -1, :], np.zeros((3, 5)))           # y-max Neumann
+    assert np.array_equal(jz[0], np.zeros((4, 5)))                  # z-min Neumann
+    assert np.array_equal(jz[-1], -p[-1])                           # z-max Dirichlet
+    coefficients = [np.full(j.shape, 3.0) for j in (jx, jy, jz)]
+    zero = [np.zeros(j.shape) for j in (jx, jy, jz)]
+    dq = pressure_steps.correct_flux(p, coefficients, zero, boundary)
+    for d, j in zip(dq, (jx, jy, jz)):
+        assert np.array_equal(d, -3.0 * j)
