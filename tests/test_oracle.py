@@ -232,6 +232,57 @@ def test_iteration_cap_publishes_nothing(algorithm):
         assert np.array_equal(xr, x0)
 
 
+def test_ibm_coarse_rows_exclude_the_solid_identity():
+    """Coarse rows of a masked hierarchy hold only the fluid cells' reaction
+    and the open faces leaving the aggregate; a fully solid aggregate is an
+    identity row (tests/unit/solver_mg_reuse_test.cpp:334-418: 16x12x8
+    cells, faces 1e-9, diagonal 7e-9, one solid cell and a solid 2x2x2
+    block)."""
+    import ref_oracle
+    nx, ny, nz = 16, 12, 8
+    scale = 1e-9
+    active = np.ones((nz, ny, nx), np.uint8)
+    active[1, 1, 1] = 0
+    active[2:4, 2:4, 2:4] = 0
+    s = _uniform_system((nx, ny, nz), 7.0 * scale, scale, active=active)
+    o = _oracle(s, ref_oracle.MgPolicy())
+    levels = o.levels()
+    if ref_oracle.available():
+        assert ref_oracle.RefSession(s, ref_oracle.MgPolicy()).levels() == levels
+
+    def open_cell(c):
+        i, j, k = c
+        inside = 0 <= i < nx and 0 <= j < ny and 0 <= k < nz
+        return not inside or active[k, j, i] != 0
+
+    width = [1, 1, 1]
+    previous = (nx, ny, nz)
+    assert len(levels) > 2
+    for level in range(1, len(levels)):
+        shape = levels[level][:3]
+        width = [w * (2 if shape[a] != previous[a] else 1) for a, w in enumerate(width)]
+        previous = shape
+        diagonal = o.level_coefficients(level)[0]
+        for x, y, z in np.ndindex(*shape):
+            parent = (x, y, z)
+            lo = [parent[a] * width[a] for a in range(3)]
+            hi = [min((parent[a] + 1) * width[a], (nx, ny, nz)[a]) for a in range(3)]
+            fluid = external = 0
+            for i, j, k in np.ndindex(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]):
+                cell = (lo[0] + i, lo[1] + j, lo[2] + k)
+                if not active[cell[2], cell[1], cell[0]]:
+                    continue
+                fluid += 1
+                for a in range(3):
+                    for step in (-1, 1):
+                        nb = list(cell)
+                        nb[a] += step
+                        if not lo[a] <= nb[a] < hi[a] and open_cell(nb):
+                            external += 1
+            expected = 1.0 if fluid == 0 else (fluid + external) * scale
+            assert abs(diagonal[z, y, x] - expected) <= 1e-14 * max(scale, expected)
+
+
 def _scalar_chebyshev(rhs, diagonal, eigenvalue, stages, fraction):
     beta = 2.0
     alpha = fraction * beta
