@@ -283,6 +283,41 @@ def test_ibm_coarse_rows_exclude_the_solid_identity():
             assert abs(diagonal[z, y, x] - expected) <= 1e-14 * max(scale, expected)
 
 
+def _box_system(n, lengths):
+    """Uniform cells on a box, Dirichlet sides, faces area / distance."""
+    nx, ny, nz = n
+    faces = tuple(np.linspace(0.0, length, m + 1) for m, length in zip(n, lengths))
+    hx, hy, hz = (length / m for m, length in zip(n, lengths))
+    fx = np.full((nz, ny, nx + 1), hy * hz / hx)
+    fy = np.full((nz, ny + 1, nx), hx * hz / hy)
+    fz = np.full((nz + 1, ny, nx), hx * hy / hz)
+    diagonal = fx[:, :, :-1] + fx[:, :, 1:] + fy[:, :-1] + fy[:, 1:] + fz[:-1] + fz[1:]
+    return workloads.PressureSystem("box", tuple(n), faces, (0,) * 6, np.ones((nz, ny, nx)),
+                                    diagonal, fx, fy, fz, None, np.zeros((nz, ny, nx)))
+
+
+def test_coarsening_selection():
+    """Strategy selection (tests/unit/solver_mg_reuse_test.cpp:414-470):
+    16x12x8 cells on the unit cube coarsen in x, y and z with point
+    smoothing; 64x48x8 cells on 1 x 1 x 4 (x and y strong) keep full
+    coarsening with alternating x/y lines down to a terminal grid of at
+    most 3 x 3 in the strong plane.  The compiled reference, when built,
+    selects the same hierarchy."""
+    import ref_oracle
+    for n, lengths in (((16, 12, 8), (1.0, 1.0, 1.0)), ((64, 48, 8), (1.0, 1.0, 4.0))):
+        s = _box_system(n, lengths)
+        levels = _oracle(s, ref_oracle.MgPolicy()).levels()
+        assert len(levels) > 1
+        assert levels[1][:3] == tuple((m + 1) // 2 for m in n)  # full x/y/z coarsening
+        if n == (16, 12, 8):
+            assert all(level[3] == 0 for level in levels)
+        else:
+            assert all(level[3] == 3 for level in levels)
+            assert levels[-1][0] <= 3 and levels[-1][1] <= 3
+        if ref_oracle.available():
+            assert ref_oracle.RefSession(s, ref_oracle.MgPolicy()).levels() == levels
+
+
 def _scalar_chebyshev(rhs, diagonal, eigenvalue, stages, fraction):
     beta = 2.0
     alpha = fraction * beta
