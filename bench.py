@@ -39,6 +39,15 @@ CONFIG_NAME = "wrinkled256"
 RTOL = 1e-10
 TRUE_RESIDUAL_INTERVAL = 4
 WARM_SEQUENCE = 20
+DATA = "synthetic (seeded SplitMix64/Box-Muller face-flux divergence)"
+
+
+def workload_label(shape):
+    """Both arms name the same workload: the stretched wrinkled-flame system
+    (256^3 unless --shape overrides it) and its warm-start sequence."""
+    nx, ny, nz = shape
+    size = f"{nx}^3" if nx == ny == nz else f"{nx}x{ny}x{nz}"
+    return f"wrinkled256 warm-start pressure solve ({size} stretched, {WARM_SEQUENCE}-step sequence)"
 
 
 def parse():
@@ -267,8 +276,8 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64/Box-Muller)",
-        "config": {"workload": "wrinkled256 warm-start pressure solve (256^3 stretched)",
+        "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": {"workload": workload_label(shape),
                    "shape": shape,
                    "algorithm": "solve_pcg + NativeCartesianMgPlan (production policy, unit_linear)",
                    "rtol": RTOL},
@@ -440,8 +449,8 @@ def run_b200(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * seconds / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded SplitMix64/Box-Muller face-flux divergence)",
-            "config": {"workload": "wrinkled256 warm-start pressure solve (256^3 stretched, 20-step sequence)",
+            "data": DATA,
+            "config": {"workload": workload_label(system.shape),
                        "shape": list(system.shape), "stretch_y": 1.02,
                        "algorithm": "PCG (solve_pcg control flow) + MG production policy, unit_linear",
                        "rtol": RTOL, "true_residual_interval": TRUE_RESIDUAL_INTERVAL,
