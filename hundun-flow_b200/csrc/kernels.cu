@@ -1055,15 +1055,19 @@ __global__ void k_beta_faces(int nx, int ny, int nz, const double* xf,
       if (is_neumann) {
         value = 0.0;
       } else {
+        // Ghost state = owner state: 2 A / (d / beta_o + d / beta_g).
         const int owner = cell(high ? n_axis - 1 : 0);
-        const double centre = 0.5 * (faces[high ? n_axis - 1 : 0] + faces[high ? n_axis : 1]);
+        const int m = high ? n_axis - 1 : 0;
+        const double centre = faces[m] + 0.5 * (faces[m + 1] - faces[m]);
         const double d = high ? faces[n_axis] - centre : centre - faces[0];
-        const double inv = 1.0 / beta[owner];
-        value = 2.0 * area / (d * inv + d * inv);
+        const double b = beta[owner];
+        value = 2.0 * area / (d / b + d / b);
       }
     } else {
-      const double cl = 0.5 * (faces[normal - 1] + faces[normal]);
-      const double cr = 0.5 * (faces[normal] + faces[normal + 1]);
+      // Cell centres as the reference's geometry compiler forms them,
+      // left + 0.5 * width (finish_axis_metrics, src/mesh_focus.cpp:584-600).
+      const double cl = faces[normal - 1] + 0.5 * (faces[normal] - faces[normal - 1]);
+      const double cr = faces[normal] + 0.5 * (faces[normal + 1] - faces[normal]);
       const double dl = faces[normal] - cl;
       const double dr = cr - faces[normal];
       value = area / (dl / beta[cell(normal - 1)] + dr / beta[cell(normal)]);

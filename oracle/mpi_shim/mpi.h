@@ -67,6 +67,9 @@ typedef void MPI_User_function(void*, void*, int*, MPI_Datatype*);
 #define MPI_UNSIGNED_LONG_LONG ((9 << 8) | 8)
 #define MPI_LONG_LONG ((10 << 8) | 8)
 #define MPI_INT64_T ((11 << 8) | 8)
+#define MPI_UINT32_T ((13 << 8) | 4)
+/* struct { double value; int index; }: 12 bytes of data padded to 16. */
+#define MPI_DOUBLE_INT ((12 << 8) | 16)
 
 #define MPI_MIN 1
 #define MPI_MAX 2
@@ -75,6 +78,8 @@ typedef void MPI_User_function(void*, void*, int*, MPI_Datatype*);
 #define MPI_LOR 5
 #define MPI_BAND 6
 #define MPI_BOR 7
+#define MPI_MAXLOC 8
+#define MPI_MINLOC 9
 
 /* Derived contiguous types: handle = 0x40000000 | table index. */
 #define HFPS_SHIM_DERIVED_BASE 0x40000000

@@ -26,6 +26,53 @@ import numpy as np
 NEUMANN = 1
 
 
+def axis_metrics(faces):
+    """(centres, widths) of one axis as the reference's geometry compiler
+    derives them (finish_axis_metrics, src/mesh_focus.cpp:584-600):
+    width = right - left, centre = left + 0.5 * width."""
+    f = np.asarray(faces, dtype=np.float64)
+    widths = f[1:] - f[:-1]
+    return f[:-1] + 0.5 * widths, widths
+
+
+def face_coefficients(beta, faces, boundary):
+    """Face coefficients of face_pressure_coefficient (src/solver_piso.cpp:
+    1060-1136) for a cell mobility beta (the reference's density * r_au):
+    interior faces A / (d_L / beta_L + d_R / beta_R) with d the centre-to-
+    face distances; a Dirichlet boundary face 2 A / (d / beta_o + d /
+    beta_g) with the ghost state equal to the owner's; Neumann 0.  A is the
+    product of the two transverse widths in the reference's order (face_area,
+    src/solver_cartesian.cpp:319-331).  Returns the x-, y-, z-face arrays."""
+    metrics = [axis_metrics(f) for f in faces]
+    (_, wx), (_, wy), (_, wz) = metrics
+    out = []
+    for axis in range(3):
+        f = np.asarray(faces[axis], dtype=np.float64)
+        centres, widths = metrics[axis]
+        if axis == 0:
+            area = (wy[:, None] * wz[None, :]).T[:, :, None]      # (nz, ny, 1)
+        elif axis == 1:
+            area = (wx[None, :] * wz[:, None])[:, None, :]        # (nz, 1, nx)
+        else:
+            area = (wx[None, :] * wy[:, None])[None, :, :]        # (1, ny, nx)
+        b = np.moveaxis(beta, 2 - axis, -1)                       # axis last
+        a = np.moveaxis(area, 2 - axis, -1)
+        dl = f[1:-1] - centres[:-1]
+        dr = centres[1:] - f[1:-1]
+        interior = a / (dl / b[..., :-1] + dr / b[..., 1:])
+        lo_d = centres[0] - f[0]
+        hi_d = f[-1] - centres[-1]
+        lo = 2.0 * a / (lo_d / b[..., :1] + lo_d / b[..., :1])
+        hi = 2.0 * a / (hi_d / b[..., -1:] + hi_d / b[..., -1:])
+        if boundary[2 * axis] == NEUMANN:
+            lo = np.zeros_like(lo)
+        if boundary[2 * axis + 1] == NEUMANN:
+            hi = np.zeros_like(hi)
+        coef = np.concatenate([lo, interior, hi], axis=-1)
+        out.append(np.ascontiguousarray(np.moveaxis(coef, -1, 2 - axis)))
+    return out
+
+
 def cell_volume(faces):
     """w_x * w_y * w_z per cell, widths as face-coordinate differences."""
     wx = np.diff(faces[0])

@@ -189,3 +189,109 @@ class RefSession:
             "recycle_cycle_corrections": int(out[14]),
         }
         return x, info
+
+
+# ---------------------------------------------------------------------------
+# The steps either side of the solve, from the reference's own sources
+# (oracle/_ref/libhfps_ref_steps.so, built from ref_pressure_steps.cpp by
+# ``make -C oracle ref``): face_pressure_coefficient, the pressure-system
+# assembly and the flux correction.  The reference's runtime-axes geometry
+# rounds every face coordinate to binary32 (copy_runtime_faces,
+# src/mesh_cartesian.cpp:344-352); ``binary32_faces`` gives coordinates that
+# survive that rounding unchanged, so both sides see the same mesh.
+
+STEPS_LIBRARY = os.path.join(HERE, "_ref", "libhfps_ref_steps.so")
+_steps = None
+
+
+def steps_available() -> bool:
+    return os.path.exists(STEPS_LIBRARY)
+
+
+def binary32_faces(faces):
+    return tuple(np.ascontiguousarray(np.asarray(f, dtype=np.float32).astype(np.float64))
+                 for f in faces)
+
+
+def _steps_lib():
+    global _steps
+    if _steps is None:
+        lib = ctypes.CDLL(STEPS_LIBRARY)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        vp = ctypes.c_void_p
+        geo = [ctypes.c_int] * 3 + [dp] * 3 + [ip]
+        lib.hfref_face_coefficients.argtypes = geo + [dp] * 4
+        lib.hfref_axis_metrics.argtypes = geo + [ctypes.c_int] + [dp] * 3
+        lib.hfref_assemble.argtypes = geo + [dp] * 6 + [ctypes.c_int] + [ctypes.c_double] * 3 + [
+            dp, dp, vp, dp, vp, dp, dp]
+        lib.hfref_correct_flux.argtypes = geo + [dp] * 4 + [ctypes.c_double] + [dp] * 3
+        _steps = lib
+    return _steps
+
+
+class RefSteps:
+    """Face coefficients, assembly and flux correction of one grid, computed
+    by the reference's code.  ``faces`` must be binary32-representable."""
+
+    def __init__(self, shape, faces, boundary):
+        self.shape = tuple(int(n) for n in shape)
+        self.faces = tuple(np.ascontiguousarray(f, dtype=np.float64) for f in faces)
+        for f in self.faces:
+            if not np.array_equal(f, f.astype(np.float32).astype(np.float64)):
+                raise ValueError("face coordinates must be binary32-representable")
+        self._bc = (ctypes.c_int * 6)(*boundary)
+        self._lib = _steps_lib()
+
+    def _geo(self):
+        nx, ny, nz = self.shape
+        return (nx, ny, nz, _dp(self.faces[0]), _dp(self.faces[1]), _dp(self.faces[2]), self._bc)
+
+    def _face_arrays(self):
+        nx, ny, nz = self.shape
+        return (np.zeros((nz, ny, nx + 1)), np.zeros((nz, ny + 1, nx)), np.zeros((nz + 1, ny, nx)))
+
+    def face_coefficients(self, beta):
+        beta = np.ascontiguousarray(beta, dtype=np.float64)
+        out = self._face_arrays()
+        rc = self._lib.hfref_face_coefficients(*self._geo(), _dp(beta), *(_dp(a) for a in out))
+        if rc != 0:
+            raise RuntimeError(f"reference face coefficients failed: {rc}")
+        return out
+
+    def axis_metrics(self, axis):
+        n = self.shape[axis]
+        faces, centres, widths = np.zeros(n + 1), np.zeros(n), np.zeros(n)
+        rc = self._lib.hfref_axis_metrics(*self._geo(), axis, _dp(faces), _dp(centres),
+                                          _dp(widths))
+        if rc != 0:
+            raise RuntimeError(f"reference metrics failed: {rc}")
+        return faces, centres, widths
+
+    def assemble(self, coefficients, fluxes, a0, a1, a2, rho, rho_n, drho_dp, rho_nm1=None,
+                 mass_source=None):
+        c = [np.ascontiguousarray(a, dtype=np.float64) for a in coefficients]
+        q = [np.ascontiguousarray(a, dtype=np.float64) for a in fluxes]
+        cells = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, rho_n, drho_dp)]
+        prev = None if rho_nm1 is None else np.ascontiguousarray(rho_nm1, dtype=np.float64)
+        src = None if mass_source is None else np.ascontiguousarray(mass_source, dtype=np.float64)
+        diag = np.zeros_like(cells[0])
+        rhs = np.zeros_like(cells[0])
+        rc = self._lib.hfref_assemble(
+            *self._geo(), *(_dp(a) for a in c), *(_dp(a) for a in q), 2 if prev is not None else 1,
+            a0, a1, a2, _dp(cells[0]), _dp(cells[1]),
+            None if prev is None else prev.ctypes.data_as(ctypes.c_void_p), _dp(cells[2]),
+            None if src is None else src.ctypes.data_as(ctypes.c_void_p), _dp(diag), _dp(rhs))
+        if rc != 0:
+            raise RuntimeError(f"reference assembly failed: {rc}")
+        return diag, rhs
+
+    def correct_flux(self, correction, coefficients, fluxes, scale=1.0):
+        p = np.ascontiguousarray(correction, dtype=np.float64)
+        c = [np.ascontiguousarray(a, dtype=np.float64) for a in coefficients]
+        q = [np.array(a, dtype=np.float64, order="C") for a in fluxes]
+        rc = self._lib.hfref_correct_flux(*self._geo(), _dp(p), *(_dp(a) for a in c), scale,
+                                          *(_dp(a) for a in q))
+        if rc != 0:
+            raise RuntimeError(f"reference flux correction failed: {rc}")
+        return q

@@ -2,7 +2,9 @@
 
 Run in a tree where the reference sources are present:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py            # small cases
+    python tests/golden/make_golden.py --scale                          # 128^3, 256^3
+    python tests/golden/make_golden.py --steps                          # assembly steps
 
 For each small case the script builds the seeded system with
 hfps.workloads, then records what the reference's own code returns for it
@@ -147,5 +149,127 @@ def main():
         json.dump(index, f, indent=1)
 
 
+# Benchmark-scale cases: the y-stretched wrinkled flame at 128^3 and at the
+# benchmarked 256^3, solved by the reference's production PCG (unit-scaled
+# MG plan) and FGMRES(12) (residual-minimising plan): the cold first solve of
+# the PISO warm-start sequence and the warm second one (rhs + 0.05 div of the
+# seed-1 noise, x0 = the reference's first PCG solution), at rtol 1e-13 and
+# at the benchmark's 1e-10.  Full solutions at these sizes are too large to
+# commit, so a fixed seeded sample of cells is recorded, together with the
+# sample's and the full vector's norms.
+SCALE_CASES = {
+    "wrinkled128": dict(config="wrinkled256", n=(128, 128, 128), stretch_y=1.02),
+    "wrinkled256": dict(config="wrinkled256", n=(256, 256, 256), stretch_y=1.02),
+}
+SCALE_SAMPLE = 32768
+
+
+def scale_sample(cells: int) -> np.ndarray:
+    rng = np.random.default_rng(2026)
+    return np.sort(rng.choice(cells, size=min(SCALE_SAMPLE, cells), replace=False))
+
+
+def _scale_solve(args):
+    """One reference solve in its own process (spawned): returns the solution
+    and the solve record."""
+    spec, algorithm, rhs_seed, x0_path, rtol = args
+    system = system_for(spec)
+    rhs = system.rhs if rhs_seed == 0 else workloads.warm_start_rhs(system, rhs_seed)
+    x0 = np.load(x0_path) if x0_path else None
+    ref = ref_oracle.RefSession(system, ref_oracle.MgPolicy.production(), algorithm=algorithm,
+                                restart=12)
+    x, info = ref.solve(rhs, x0=x0, rtol=rtol, maxit=400)
+    ref.close()
+    return x, info
+
+
+def scale_main(names, workdir):
+    import multiprocessing as mp
+    os.makedirs(workdir, exist_ok=True)
+    ctx = mp.get_context("spawn")
+    for name in names:
+        spec = SCALE_CASES[name]
+        system = system_for(spec)
+        cells = scale_sample(system.cells)
+        ref = ref_oracle.RefSession(system, ref_oracle.MgPolicy.production(), algorithm="pcg")
+        levels = ref.levels()
+        mg = ref.apply_mg(probe_vector(system)).reshape(-1)
+        ref.close()
+        entry = {"spec": spec, "digest": input_digest(system), "levels": levels,
+                 "sample_cells": int(cells.size), "sample_seed": 2026}
+        arrays = {"cells": cells, "mg": mg[cells]}
+        cold = [(spec, a, 0, None, rtol) for a in ("pcg", "fgmres") for rtol in (1e-13, 1e-10)]
+        with ctx.Pool(len(cold)) as pool:
+            results = pool.map(_scale_solve, cold)
+        p0 = results[0][0]
+        x0_path = os.path.join(workdir, f"{name}_p0.npy")
+        np.save(x0_path, p0)
+        warm = [(spec, a, 1, x0_path, rtol) for a in ("pcg", "fgmres") for rtol in (1e-13, 1e-10)]
+        with ctx.Pool(len(warm)) as pool:
+            results += pool.map(_scale_solve, warm)
+        for (args, (x, info)) in zip(cold + warm, results):
+            _, algorithm, step, _, rtol = args
+            key = f"{algorithm}_step{step}_{'1e13' if rtol < 1e-11 else '1e10'}"
+            flat = x.reshape(-1)
+            arrays[key] = flat[cells]
+            entry[key] = {"iterations": info["iterations"], "termination": info["termination"],
+                          "final_true_residual": info["final_true_residual"],
+                          "rhs_norm": info["rhs_norm"],
+                          "norm": float(np.linalg.norm(flat)),
+                          "operator_applies": info["operator_applies"]}
+            print(name, key, info["iterations"], info["termination"], flush=True)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **arrays)
+        with open(os.path.join(HERE, f"{name}.json"), "w") as f:
+            json.dump(entry, f, indent=1)
+
+
+def steps_main():
+    """Face coefficients (face_pressure_coefficient), the assembled system
+    (assemble_pressure_system_impl) and corrected fluxes
+    (PressureCorrectionBoundaryPlan::mass_flux_response) from the reference's
+    code (oracle/_ref/libhfps_ref_steps.so) on the cases of
+    tests/golden_cases.py STEPS_CASES."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    import golden_cases
+    if not ref_oracle.steps_available():
+        raise SystemExit("build oracle/_ref first: make -C oracle ref")
+    arrays, index = {}, {}
+    for name in golden_cases.STEPS_CASES:
+        s, faces = golden_cases.steps_system(name)
+        ref = ref_oracle.RefSteps(s.shape, faces, s.boundary)
+        coefficients = ref.face_coefficients(s.beta)
+        for axis, c in zip("xyz", coefficients):
+            arrays[f"{name}_face_{axis}"] = c
+        inp = golden_cases.steps_inputs(s, 4)
+        for tag, (a0, a1, a2, bdf2) in golden_cases.STEPS_BDF.items():
+            diag, rhs = ref.assemble(coefficients, inp["fluxes"], a0, a1, a2, inp["rho"],
+                                     inp["rho_n"], inp["drho_dp"],
+                                     rho_nm1=inp["rho_nm1"] if bdf2 else None,
+                                     mass_source=inp["mass_source"] if bdf2 else None)
+            arrays[f"{name}_{tag}_diag"] = diag
+            arrays[f"{name}_{tag}_rhs"] = rhs
+        for scale in golden_cases.STEPS_SCALES:
+            q = ref.correct_flux(inp["correction"], coefficients, inp["fluxes"], scale)
+            for axis, f in zip("xyz", q):
+                arrays[f"{name}_flux_{scale}_{axis}"] = f
+        index[name] = {"digest": input_digest(s), "shape": list(s.shape)}
+        print(name, "recorded")
+    np.savez_compressed(os.path.join(HERE, "pressure_steps.npz"), **arrays)
+    with open(os.path.join(HERE, "pressure_steps.json"), "w") as f:
+        json.dump(index, f, indent=1)
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "--steps":
+        steps_main()
+        raise SystemExit(0)
+    if not ref_oracle.available():
+        raise SystemExit("build oracle/_ref first: make -C oracle ref")
+    if len(sys.argv) > 1 and sys.argv[1] == "--scale":
+        # python tests/golden/make_golden.py --scale [names...]; the warm
+        # start vectors go to a scratch folder (HFPS_GOLDEN_SCRATCH, default
+        # /tmp/hfps_golden).
+        scale_main(sys.argv[2:] or list(SCALE_CASES),
+                   os.environ.get("HFPS_GOLDEN_SCRATCH", "/tmp/hfps_golden"))
+    else:
+        main()

@@ -75,3 +75,46 @@ def line_relaxation_policy(lines=True):
     import ref_oracle
     return ref_oracle.MgPolicy(smoother=1, cycle=0, pre=1, post=1, coarse_sweeps=16,
                                max_levels=12, anisotropy_threshold=4.0 if lines else 1e300)
+
+
+# ---- steps either side of the solve (tests/golden/pressure_steps.*) -------
+STEPS_CASES = {
+    # name: workloads config and overrides
+    "wrinkled_20x28x12": dict(config="wrinkled256", n=(20, 28, 12), stretch_y=1.05, seed=9),
+    "sphere_14x11x9": dict(config="sphere64", n=(14, 11, 9), seed=6),
+}
+
+
+def steps_system(name):
+    """The case's system with binary32-representable face coordinates (the
+    reference's runtime-axes geometry rounds every coordinate to binary32)."""
+    from hfps import workloads
+    import ref_oracle
+    spec = dict(STEPS_CASES[name])
+    cfg = spec.pop("config")
+    s = workloads.make(cfg, **spec)
+    return s, ref_oracle.binary32_faces(s.faces)
+
+
+def steps_inputs(s, seed):
+    """Seeded cell states and face fluxes of one assembly / correction case."""
+    rng = np.random.default_rng(seed)
+    shape = s.rhs.shape
+    return {
+        "rho": 1.0 + rng.random(shape),
+        "rho_n": 1.0 + rng.random(shape),
+        "drho_dp": 0.2 + rng.random(shape),
+        "rho_nm1": 1.0 + rng.random(shape),
+        "mass_source": 0.1 * rng.standard_normal(shape),
+        "fluxes": [rng.standard_normal(f.shape) for f in (s.face_x, s.face_y, s.face_z)],
+        "correction": rng.standard_normal(shape),
+    }
+
+
+# (a0, a1, a2, BDF2 with a mass source)
+STEPS_BDF = {"bdf1": (1.0, -1.0, 0.0, False), "bdf2_source": (1.5, -2.0, 0.5, True)}
+STEPS_SCALES = (1.0, 0.7)
+
+
+def steps_arrays():
+    return dict(np.load(os.path.join(GOLDEN, "pressure_steps.npz")))

@@ -123,3 +123,40 @@ def test_corrected_flux_closes_continuity(hfps_mod):
     residual = (volume * (inp["density_trial"] - inp["density_accepted"]) + storage * p +
                 pressure_steps.outward_flux(*q))
     assert np.linalg.norm(residual) <= 1e-10 * np.linalg.norm(rhs)
+
+
+# ---- pinned to the reference's own code (tests/golden/pressure_steps.*) ----
+STEPS_NAMES = ["sphere_14x11x9", "wrinkled_20x28x12"]
+
+
+@pytest.mark.parametrize("name", STEPS_NAMES)
+def test_steps_match_reference_record(hfps_mod, name):
+    """hfps_set_beta's faces, hfps_assemble's system and hfps_correct_flux's
+    fluxes equal what the reference's face_pressure_coefficient,
+    assemble_pressure_system_impl and mass_flux_response returned on the same
+    binary32 mesh, bit for bit."""
+    import golden_cases
+    s, faces = golden_cases.steps_system(name)
+    ref = golden_cases.steps_arrays()
+    policy = hfps_mod.Policy.production()
+    g = hfps_mod.PressureSolver(s.shape, faces, s.boundary, None, policy=policy)
+    g.set_beta(np.ascontiguousarray(s.beta))
+    _, fx, fy, fz, _ = g.level_coefficients(0)
+    for axis, c in zip("xyz", (fx, fy, fz)):
+        assert np.array_equal(c, ref[f"{name}_face_{axis}"]), axis
+    inp = golden_cases.steps_inputs(s, 4)
+    for tag, (a0, a1, a2, bdf2) in golden_cases.STEPS_BDF.items():
+        rhs = g.assemble(np.ascontiguousarray(s.beta), inp["rho"], inp["rho_n"], inp["drho_dp"],
+                         inp["fluxes"], a0, a1, a2,
+                         density_previous=inp["rho_nm1"] if bdf2 else None,
+                         mass_source=inp["mass_source"] if bdf2 else None)
+        diag, *_ = g.level_coefficients(0)
+        assert np.array_equal(diag, ref[f"{name}_{tag}_diag"]), tag
+        assert np.array_equal(rhs, ref[f"{name}_{tag}_rhs"]), tag
+    coefficients = tuple(ref[f"{name}_face_{axis}"] for axis in "xyz")
+    for scale in golden_cases.STEPS_SCALES:
+        q = [f.copy() for f in inp["fluxes"]]
+        g.correct_flux(inp["correction"], coefficients, q, scale)
+        for axis, f in zip("xyz", q):
+            assert np.array_equal(f, ref[f"{name}_flux_{scale}_{axis}"]), (scale, axis)
+    g.close()
