@@ -161,12 +161,15 @@ SCALE_CASES = {
     "wrinkled128": dict(config="wrinkled256", n=(128, 128, 128), stretch_y=1.02),
     "wrinkled256": dict(config="wrinkled256", n=(256, 256, 256), stretch_y=1.02),
 }
-SCALE_SAMPLE = 32768
+SCALE_SAMPLE = 8192
 
 
 def scale_sample(cells: int) -> np.ndarray:
+    """Every fourth of 32768 distinct cells drawn with seed 2026, in
+    increasing order (8192 cells, about 0.05% of the 256^3 grid)."""
     rng = np.random.default_rng(2026)
-    return np.sort(rng.choice(cells, size=min(SCALE_SAMPLE, cells), replace=False))
+    drawn = np.sort(rng.choice(cells, size=min(4 * SCALE_SAMPLE, cells), replace=False))
+    return drawn[::4]
 
 
 def _scale_solve(args):
