@@ -5,6 +5,7 @@ Run in a tree where the reference sources are present:
     make -C oracle ref && python tests/golden/make_golden.py            # small cases
     python tests/golden/make_golden.py --scale                          # 128^3, 256^3
     python tests/golden/make_golden.py --steps                          # assembly steps
+    python tests/golden/make_golden.py --c2                             # 512x256x256
 
 For each small case the script builds the seeded system with
 hfps.workloads, then records what the reference's own code returns for it
@@ -226,6 +227,35 @@ def scale_main(names, workdir):
             json.dump(entry, f, indent=1)
 
 
+def c2_main(workdir):
+    """The mixed-precision configuration's system (512x256x256 wrinkled
+    flame, uniform cells, point Chebyshev smoothing): the reference's cold
+    PCG solve at rtol 1e-13 and 1e-10 (tests/golden/wrinkled512x256x256.*),
+    the FP64 oracle solution the mixed form's error is measured against."""
+    import multiprocessing as mp
+    os.makedirs(workdir, exist_ok=True)
+    spec = dict(config="wrinkled512x256x256")
+    system = system_for(spec)
+    cells = scale_sample(system.cells)
+    entry = {"spec": spec, "digest": input_digest(system), "sample_cells": int(cells.size),
+             "sample_seed": 2026}
+    arrays = {"cells": cells}
+    jobs = [(spec, "pcg", 0, None, rtol) for rtol in (1e-13, 1e-10)]
+    with mp.get_context("spawn").Pool(len(jobs)) as pool:
+        results = pool.map(_scale_solve, jobs)
+    for (args, (x, info)) in zip(jobs, results):
+        key = f"pcg_step0_{'1e13' if args[4] < 1e-11 else '1e10'}"
+        flat = x.reshape(-1)
+        arrays[key] = flat[cells]
+        entry[key] = {"iterations": info["iterations"], "termination": info["termination"],
+                      "final_true_residual": info["final_true_residual"],
+                      "rhs_norm": info["rhs_norm"], "norm": float(np.linalg.norm(flat))}
+        print("wrinkled512x256x256", key, info["iterations"], info["termination"], flush=True)
+    np.savez_compressed(os.path.join(HERE, "wrinkled512x256x256.npz"), **arrays)
+    with open(os.path.join(HERE, "wrinkled512x256x256.json"), "w") as f:
+        json.dump(entry, f, indent=1)
+
+
 def steps_main():
     """Face coefficients (face_pressure_coefficient), the assembled system
     (assemble_pressure_system_impl) and corrected fluxes
@@ -265,6 +295,9 @@ def steps_main():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "--steps":
         steps_main()
+        raise SystemExit(0)
+    if len(sys.argv) > 1 and sys.argv[1] == "--c2":
+        c2_main(os.environ.get("HFPS_GOLDEN_SCRATCH", "/tmp/hfps_golden"))
         raise SystemExit(0)
     if not ref_oracle.available():
         raise SystemExit("build oracle/_ref first: make -C oracle ref")
