@@ -72,7 +72,9 @@ k_operator_dot_noalloc(Level<double> L, const double* __restrict__ x,
   }
 }
 
-// Scratch address per device, looked up once with that device current.
+// Scratch address per device, looked up once with that device current.  The
+// address belongs to the device's primary context: cudaDeviceReset discards
+// it together with the module, so the cached value is void afterwards.
 std::mutex g_setup_mutex;
 double* g_scratch_address[kMaxDevices] = {};
 
@@ -142,6 +144,13 @@ extern "C" HFPS_API int hfps_operator_dot_noalloc(const hfps_operator_view* op,
   const std::uintptr_t yb = reinterpret_cast<std::uintptr_t>(y);
   const std::uintptr_t bytes = static_cast<std::uintptr_t>(n) * sizeof(double);
   if (xb < yb + bytes && yb < xb + bytes) return HFPS_INVALID_PLAN;
+  // The dot is written after the sweep: inside x or y it would overwrite
+  // one input value or one result row.
+  if (x_dot_y != nullptr) {
+    const std::uintptr_t db = reinterpret_cast<std::uintptr_t>(x_dot_y);
+    const std::uintptr_t de = db + sizeof(double);
+    if ((db < xb + bytes && xb < de) || (db < yb + bytes && yb < de)) return HFPS_INVALID_PLAN;
+  }
 
   Level<double> L{op->nx, op->ny, op->nz, neumann, op->diagonal,
                   op->face_x, op->face_y, op->face_z, nullptr};

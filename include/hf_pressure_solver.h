@@ -337,14 +337,18 @@ HFPS_API int hfps_profile_kernel(hfps_solver* solver, int kernel,
  *
  * The first call on each device does a one-time set-up: it looks up the
  * address of the library's scratch array on that device.  Make that first
- * call before any stream capture begins.  The scratch array is shared by
- * every call on a device, so calls that overlap in time (two streams, two
- * host threads) race and give wrong results: serialise them.
+ * call before any stream capture begins.  The looked-up address is kept for
+ * the life of the process; cudaDeviceReset on a device voids it, so after a
+ * reset this entry point must not be called on that device again.  The
+ * scratch array is shared by every call on a device, so calls that overlap
+ * in time (two streams, two host threads) race and give wrong results:
+ * serialise them.
  *
  * Returns HFPS_OK, HFPS_INVALID_CASE when an extent is below 1 or the grid
  * has more than HFPS_NOALLOC_MAX_CELLS cells, or HFPS_INVALID_PLAN for a
  * periodic or unknown boundary kind, a NULL, misaligned or non-device
- * pointer, y overlapping x, or a CUDA runtime error. */
+ * pointer, y overlapping x, x_dot_y inside x or y, or a CUDA runtime
+ * error. */
 #define HFPS_NOALLOC_MAX_CELLS (1LL << 30)   /* 32-bit face indexing */
 #define HFPS_NOALLOC_MAX_BLOCKS 1184         /* reduction partials kept */
 

@@ -5,8 +5,10 @@ its reduction scratch in a fixed device array inside the library.  Two calls
 in a row on the same device must each give the y = A x that
 hfps_apply_operator gives for the same coefficients (bit-identical rows:
 same arithmetic order, FMA contraction off) and x.(A x) to 1e-12 relative.
-The file is named to be collected last, so it also runs after every other
-GPU test in the same process.
+The second call must leave the device's free memory unchanged: the first
+call has already loaded the module and looked up the scratch address, so
+nothing is left that could allocate.  The file is named to be collected
+last, so it also runs after every other GPU test in the same process.
 """
 import ctypes
 
@@ -66,10 +68,13 @@ def test_noalloc_matches_operator_twice(hfps_mod, shape):
         xd = torch.from_numpy(x).cuda()
         yd = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
         dot = torch.full((1,), np.nan, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         assert noalloc(view, xd, yd, dot) == 0, call
+        if call == 1:
+            assert torch.cuda.mem_get_info()[0] == free_before
         y = yd.cpu().numpy()
-        scale = np.max(np.abs(expect))
-        assert np.max(np.abs(y - expect)) <= 1e-15 * scale, call
+        assert np.array_equal(y, expect), call
         want = float(np.dot(x, expect))
         assert abs(float(dot.item()) - want) <= 1e-12 * abs(want), call
 
@@ -90,9 +95,12 @@ def test_noalloc_rejects_bad_arguments(hfps_mod):
     host = torch.zeros(n, dtype=torch.float64)
     assert noalloc(view, xd, host, None) == 2      # host output
     assert noalloc(view, xd, xd, None) == 2        # y aliases x
+    assert noalloc(view, xd, yd, xd[3:4]) == 2     # dot written into x
+    assert noalloc(view, xd, yd, yd[n - 1:]) == 2  # dot written into y
     view.boundary[0] = 2
     assert noalloc(view, xd, yd, None) == 2        # periodic
     view.boundary[0] = int(s.boundary[0])
     assert noalloc(view, xd, yd, None) == 0
     expect = g.apply_operator(np.ones(s.rhs.shape)).reshape(-1)
-    assert np.max(np.abs(yd.cpu().numpy() - expect)) <= 1e-15 * np.max(np.abs(expect))
+    assert np.array_equal(yd.cpu().numpy(), expect)
+    assert torch.equal(xd, torch.ones(n, dtype=torch.float64, device="cuda"))
