@@ -18,7 +18,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIBRARY = os.path.join(HERE, "libhfps.so")
-SOURCES = ["kernels.cu", "kernels_line.cu", "solver.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["kernels.cu", "kernels_line.cu", "kernels_tail.cu", "solver.cu", "capi.cu",
+           "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr",
@@ -69,6 +70,24 @@ def build(verbose: bool = False, force: bool = False) -> str:
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIBRARY, *objects, "-lcudart"]
         run(cmd)
     return LIBRARY
+
+
+# The C++ torch extension of the differentiable solve (csrc/torch_autograd.cpp,
+# used for gradient checks).  It calls only the C ABI, links libhfps.so and is
+# built in-tree into hfps/_ext/ (which travels with the checkout).
+TORCH_EXT_DIR = os.path.join(HERE, "hfps", "_ext")
+
+
+def build_torch_extension(verbose: bool = False):
+    """Compiles (when stale) and imports the extension module."""
+    from torch.utils.cpp_extension import load
+    os.makedirs(TORCH_EXT_DIR, exist_ok=True)
+    return load(name="hfps_torch_autograd",
+                sources=[os.path.join(CSRC, "torch_autograd.cpp")],
+                extra_include_paths=[os.path.join(ROOT, "include")],
+                extra_cflags=["-O2"],
+                extra_ldflags=[f"-L{HERE}", "-lhfps", f"-Wl,-rpath,{HERE}"],
+                build_directory=TORCH_EXT_DIR, verbose=verbose)
 
 
 if __name__ == "__main__":
