@@ -4,7 +4,8 @@ sizes; the small-size parity tests pin the arithmetic).
 
 * 512x256x256 wrinkled flame: the mixed-precision form (FP32 MG inside FP64
   PCG) reaches the FP64 tolerance, and its solution agrees with the plain
-  FP64 GPU solve; the refinement (Krylov) step counts are reported.
+  FP64 GPU solve and, at 1e-13, with the compiled reference's FP64 solution
+  (recorded sample); the refinement (outer Krylov) step counts are reported.
 * 128^3 spherical flame, loss L = 0.5 sum_fluid (p - p_t)^2 with p_t from
   seed 7: adjoint gradients with respect to 200 face coefficients (seed 11)
   and to rhs agree with central finite differences of step 1e-6 |c| to 1e-6
@@ -46,6 +47,21 @@ def test_mixed_form_at_512x256x256(hfps_mod):
           f"refinement steps, mixed vs FP64 relative error {err:.3e}")
     assert err <= 1e-8
     assert abs(im["iterations"] - i64["iterations"]) <= max(2, int(0.2 * i64["iterations"]))
+    # Final error against the FP64 oracle: the compiled reference's solve of
+    # this system at 1e-13 (tests/golden/wrinkled512x256x256.*), on its
+    # recorded sample of cells; the mixed form converged to the same FP64
+    # true residual.
+    import scale_cases
+    entry = scale_cases.entry("wrinkled512x256x256")
+    ref = scale_cases.arrays("wrinkled512x256x256")
+    xr, ir = g.solve(rhs, rtol=1e-13, maxit=400, precision=hfps_mod.MIXED, history=False)
+    assert ir["termination"] == "converged"
+    oracle_err = scale_cases.sample_error(xr.cpu().numpy(), ref["pcg_step0_1e13"], ref["cells"])
+    want = entry["pcg_step0_1e13"]["iterations"]
+    print(f"512x256x256 mixed at 1e-13: {ir['iterations']} refinement steps (reference PCG "
+          f"{want}), relative error vs the reference FP64 solution {oracle_err:.3e}")
+    assert oracle_err <= 1e-9
+    assert abs(ir["iterations"] - want) <= max(2, 0.2 * want)
 
 
 def _face_vectors(s, axis, flat):
@@ -121,3 +137,50 @@ def test_adjoint_gradients_at_128(hfps_mod, precision):
         w, _ = g.solve(e.reshape(s.rhs.shape), rtol=1e-13, maxit=800)
         fd_k = float(np.sum(dl_dp * w))
         assert abs(float(lam.reshape(-1)[k]) - fd_k) <= 1e-6 * float(np.abs(lam).max())
+
+
+def test_three_spheres512_forward_adjoint_steps(hfps_mod):
+    """512^3 three-sphere flame (134M cells): the first two steps of the
+    warm-started sequence, each a mixed forward solve followed by a mixed
+    adjoint solve of L = 0.5 sum_fluid (p - p_t)^2 (p_t from seed 7).  The
+    last step is repeated in plain FP64 from the same warm start: forward
+    solutions, adjoint states and face gradients of the two forms agree."""
+    import torch
+    s = workloads.make("three_spheres512")
+    g = hfps_mod.PressureSolver.from_system(s, hfps_mod.Policy.production())
+    n = s.cells
+    rhs0 = torch.from_numpy(s.rhs.reshape(-1)).cuda()
+    active = torch.from_numpy(s.active.reshape(-1).astype(np.bool_)).cuda()
+    target = workloads.normals_torch(7, n)
+    mixed = hfps_mod.SolveOptions(rtol=1e-10, maxit=400, precision=hfps_mod.MIXED)
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    start, mid, stop = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    for step in range(2):
+        rhs = rhs0 + workloads.flux_divergence_rhs_torch(1 + step, s.faces, s.boundary,
+                                                         s.active, 0.05)
+        x_start = x.clone()
+        torch.cuda.synchronize()
+        start.record()
+        x, info = g.solve(rhs, x0=x, out=x, options=mixed, history=False)
+        mid.record()
+        dl_dp = torch.where(active, x - target, torch.zeros_like(x))
+        lam, grads, ainfo = g.adjoint(x, dl_dp, options=mixed)
+        stop.record()
+        torch.cuda.synchronize()
+        assert info["termination"] == ainfo["termination"] == "converged"
+        assert info["final_true_residual"] <= 1e-10 * info["rhs_norm"]
+        print(f"512^3 step {step + 1}: mixed forward {start.elapsed_time(mid):.1f} ms "
+              f"({info['iterations']} iterations), adjoint {mid.elapsed_time(stop):.1f} ms "
+              f"({ainfo['iterations']} iterations)")
+    x64, i64 = g.solve(rhs, x0=x_start, rtol=1e-10, maxit=400, history=False)
+    lam64, grads64, _ = g.adjoint(x, dl_dp, rtol=1e-10, maxit=400)
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+    forward = rel(x, x64)
+    adjoint = rel(lam, lam64)
+    faces = max(rel(a, b) for a, b in zip(grads, grads64))
+    print(f"512^3: FP64 forward {i64['iterations']} iterations; mixed vs FP64: solution "
+          f"{forward:.2e}, lambda {adjoint:.2e}, face gradients {faces:.2e}")
+    assert forward <= 1e-8 and adjoint <= 1e-8 and faces <= 1e-8
