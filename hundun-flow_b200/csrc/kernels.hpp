@@ -27,9 +27,18 @@ struct Scalars {
   double mg_alpha;   // MG correction scale
   double misc[4];
   double hcol[72];   // FGMRES: projections of the current column and |w|^2
-  int flags;         // bit 0 non-finite, bit 1 breakdown, bit 2 invalid assembly input
+  int flags;         // bit 0 non-finite, bit 1 breakdown, bit 2 invalid assembly input,
+                     // bit 3 a grid barrier of the small-level kernel timed out
   unsigned marks;    // bit 0: a difference had a nonzero entry (recycle capture)
   unsigned counters[8];  // last-block arrival counters, one per reduction
+  // The small-level kernel's grid barrier: arrivals and completed barriers,
+  // 128 bytes apart so that polling the one does not slow the atomics on the
+  // other.
+  unsigned tail_pad0[32];
+  unsigned tail_count;
+  unsigned tail_pad1[31];
+  unsigned tail_generation;
+  unsigned tail_pad2[31];
 };
 
 enum ScalarOp : int {
@@ -129,6 +138,46 @@ template <class T, class TC>
 void launch_coarse_solve(cudaStream_t s, const Level<TC>& L, T* x, const T* b,
                          TC* xs, TC* bs, TC* work, TC* dprime, int sweeps,
                          int line_axis);
+
+// ---- small levels as one persistent launch (kernels_tail.cu) ---------------
+// A program of cycle phases for the levels below the scan levels, executed
+// by one cooperative launch with a bounded grid barrier between phases.
+enum TailKind : int { kTailPcr = 0, kTailRestrict = 1, kTailProlong = 2, kTailDense = 3 };
+struct TailOp {
+  int kind;
+  int level;   // index into TailProgram::levels (the fine level of a transfer)
+  int arg;     // PCR: colour; transfers: coarsening mask; dense: x is zero
+  int pad;
+  // PCR: x, rhs, factors.  Restrict: fine x, fine b, coarse b, coarse x.
+  // Prolong: fine x, coarse x.  Dense: x, b, out.
+  void* p0;
+  void* p1;
+  void* p2;
+  void* p3;
+};
+constexpr int kTailMaxOps = 480;
+constexpr int kTailMaxLevels = 8;
+// Passed by value as the kernel parameter (kept under the 32 KB limit).
+template <class T>
+struct TailProgram {
+  int count;
+  int dense_n;
+  int axis[kTailMaxLevels];
+  Level<T> levels[kTailMaxLevels];
+  const double* dense_op;
+  Scalars* scalars;
+  TailOp ops[kTailMaxOps];
+};
+static_assert(sizeof(TailProgram<double>) < 32000, "kernel parameter limit");
+// log2 of the PCR width for lines of `extent` cells, or -1 if unsupported.
+int tail_steps(int extent);
+// Lines of one PCR pass a CTA of the persistent launch relaxes at once.
+int tail_lines_per_cta(int steps);
+// CTAs that can be co-resident on `sms` SMs (0: cannot run).
+template <class T>
+int tail_grid(int steps, int dense_n, int sms);
+template <class T>
+bool launch_tail(cudaStream_t s, const TailProgram<T>& prog, int steps, int blocks);
 
 // ---- MG entry/exit ------------------------------------------------------
 // b = active ? r : 0 (converted to T), and x = 0 when zero_x; b and x in

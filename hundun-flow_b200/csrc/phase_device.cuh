@@ -353,33 +353,37 @@ __device__ __forceinline__ void coarse_point_sweeps(const Level<TC>& L, TC* xw, 
 constexpr int kDenseWarps = 32;
 constexpr int kDenseUnroll = 8;
 
-template <class T>
+// WARPS: the CTA's warps (kDenseWarps for k_coarse_dense; the persistent
+// small-level kernel runs it with fewer).  part has WARPS * 32 doubles; the
+// CTA is synchronised again before return, so part may be reused at once.
+template <class T, int WARPS = kDenseWarps>
 __device__ __forceinline__ void dense_rows(int n, const double* __restrict__ op,
                                            const double* v, double* part, int vblock,
                                            int lane, int warp, bool x_zero, T* out) {
   const int row = min(vblock * 32 + lane, n - 1);
   const int cols = 2 * n;
   int first = warp;
-  if (x_zero && n > warp) first += ((n - warp + kDenseWarps - 1) / kDenseWarps) * kDenseWarps;
+  if (x_zero && n > warp) first += ((n - warp + WARPS - 1) / WARPS) * WARPS;
   double acc = 0.0;
-  for (int j0 = first; j0 < cols; j0 += kDenseWarps * kDenseUnroll) {
+  for (int j0 = first; j0 < cols; j0 += WARPS * kDenseUnroll) {
     double m[kDenseUnroll];
 #pragma unroll
     for (int u = 0; u < kDenseUnroll; ++u) {
-      const int j = min(j0 + u * kDenseWarps, cols - 1);
+      const int j = min(j0 + u * WARPS, cols - 1);
       m[u] = __ldg(op + static_cast<size_t>(j) * n + row);
     }
 #pragma unroll
     for (int u = 0; u < kDenseUnroll; ++u)
-      if (j0 + u * kDenseWarps < cols) acc += m[u] * v[j0 + u * kDenseWarps];
+      if (j0 + u * WARPS < cols) acc += m[u] * v[j0 + u * WARPS];
   }
   part[warp * 32 + lane] = acc;
   __syncthreads();
   if (warp == 0 && vblock * 32 + lane < n) {
     double sum = part[lane];
-    for (int w = 1; w < kDenseWarps; ++w) sum += part[w * 32 + lane];
+    for (int w = 1; w < WARPS; ++w) sum += part[w * 32 + lane];
     out[vblock * 32 + lane] = static_cast<T>(sum);
   }
+  __syncthreads();
 }
 
 }  // namespace hfps

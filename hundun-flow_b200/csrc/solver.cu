@@ -18,6 +18,8 @@ constexpr uint32_t kDetailPlan = 9101U;
 constexpr uint32_t kDetailCuda = 9102U;
 constexpr uint32_t kDetailNumeric = 9103U;
 constexpr uint32_t kDetailBreakdown = 9104U;
+// Whether the small levels run as one persistent launch when HFPS_TAIL is unset.
+constexpr bool kTailDefault = false;
 
 size_t align_up(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
@@ -124,6 +126,7 @@ Solver::~Solver() {
   clear_mg_graphs();
   if (dic_graph_ != nullptr) cudaGraphExecDestroy(dic_graph_);
   if (h_scalars_ != nullptr) cudaFreeHost(h_scalars_);
+  if (scalars_ready_ != nullptr) cudaEventDestroy(scalars_ready_);
   if (arena_ != nullptr) cudaFree(arena_);
   if (fg_storage_ != nullptr) cudaFree(fg_storage_);
   if (rc_storage_ != nullptr) cudaFree(rc_storage_);
@@ -345,7 +348,13 @@ Status Solver::allocate() {
     // separate dot kernel).
     const char* env = std::getenv("HFPS_KRYLOV_FUSION");
     krylov_fusion_ = !(env != nullptr && env[0] == '0');
+    // PCG queue-ahead of the next MG application (HFPS_QUEUE_AHEAD=0: the
+    // host reads each iteration's scalars before queueing more work).
+    const char* ahead = std::getenv("HFPS_QUEUE_AHEAD");
+    queue_ahead_ = !(ahead != nullptr && ahead[0] == '0');
   }
+  st = check(cudaEventCreateWithFlags(&scalars_ready_, cudaEventDisableTiming), "event");
+  if (!st) return st;
   d_scalars_ = reinterpret_cast<Scalars*>(at(scalars_off));
   d_partials_ = reinterpret_cast<double*>(at(partials_off));
   coarse_op_ = dense_off == SIZE_MAX ? nullptr : reinterpret_cast<double*>(at(dense_off));
@@ -481,6 +490,7 @@ Status Solver::build_hierarchy() {
   }
   Status st = check(cudaGetLastError(), "hierarchy kernels");
   if (!st) return st;
+  select_tail();
   // Diagonal shortcut (select_diagonal_shortcut, src/solver_mg.cpp:1577-1611).
   diagonal_shortcut_ = false;
   if (policy_.diagonal_shortcut_maximum_ratio != 0.0) {
@@ -782,6 +792,107 @@ void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels, bool x_zero) {
   }
 }
 
+// The persistent small-level launch covers levels tail_level_.. when every
+// non-coarsest one relaxes lines along one axis with PCR (few lines per
+// colour), all have the same line length, and the coarsest is the dense
+// affine map.  HFPS_TAIL=1 / 0 turns it on / off (default kTailDefault);
+// HFPS_TAIL_BLOCKS overrides its CTA count (clamped to what is co-resident).
+void Solver::select_tail() {
+  tail_level_ = -1;
+  const char* env = std::getenv("HFPS_TAIL");
+  const bool on = env != nullptr && env[0] != '\0' ? env[0] != '0' : kTailDefault;
+  if (!on || !coarse_dense_) return;
+  const int levels = static_cast<int>(l64_.size());
+  int first = levels - 1;
+  int axis = -1, extent = -1;
+  for (int l = levels - 2; l >= 1; --l) {
+    const DeviceLevel<double>& L = l64_[l];
+    const int mask = L.line_mask;
+    if (mask == 0 || (mask & (mask - 1)) != 0) break;
+    const int a = mask == 1 ? 0 : (mask == 2 ? 1 : 2);
+    if (line_kind(L.nx, L.ny, L.nz, a) != kLinePcr) break;
+    const int e = a == 0 ? L.nx : (a == 1 ? L.ny : L.nz);
+    if (axis >= 0 && (a != axis || e != extent)) break;
+    axis = a;
+    extent = e;
+    first = l;
+  }
+  if (first >= levels - 1 || levels - first > kTailMaxLevels) return;
+  const int steps = tail_steps(extent);
+  if (steps < 0) return;
+  int device = 0, sms = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const DeviceLevel<double>& top = l64_[first];
+  const int a_extent = axis == 0 ? top.ny : top.nx;
+  const int b_extent = axis == 2 ? top.ny : top.nz;
+  const int lines = ((a_extent + 1) / 2) * b_extent;
+  const int dense_n = l64_.back().cells();
+  // Enough CTAs for one round of the top level's lines (tail_lines_per_cta
+  // at a time) and for the dense map's 32-row blocks.
+  const int per_cta = tail_lines_per_cta(steps);
+  int want = std::max((lines + per_cta - 1) / per_cta, (dense_n + 31) / 32);
+  const char* blocks_env = std::getenv("HFPS_TAIL_BLOCKS");
+  if (blocks_env != nullptr && std::atoi(blocks_env) > 0) want = std::atoi(blocks_env);
+  tail_blocks_[0] = std::min(tail_grid<double>(steps, dense_n, sms), want);
+  tail_blocks_[1] = std::min(tail_grid<float>(steps, dense_n, sms), want);
+  if (tail_blocks_[0] < 1 || tail_blocks_[1] < 1) return;
+  tail_level_ = first;
+  tail_steps_ = steps;
+}
+
+template <class T>
+void Solver::tail_cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter,
+                        bool x_zero, TailProgram<T>& prog) {
+  const auto add = [&](int kind, int lv, int arg, const void* a, const void* b,
+                       const void* c, const void* d) {
+    if (prog.count >= kTailMaxOps) {
+      prog.count = kTailMaxOps + 1;  // marks an overflow; tail_launch falls back
+      return;
+    }
+    prog.ops[prog.count++] = TailOp{kind, lv - tail_level_, arg, 0, const_cast<void*>(a),
+                                    const_cast<void*>(b), const_cast<void*>(c),
+                                    const_cast<void*>(d)};
+  };
+  DeviceLevel<T>& L = levels[level];
+  if (level + 1 == static_cast<int>(levels.size())) {
+    // coarse_solve's dense branch: out = P x + M b into t, then x <-> t.
+    add(kTailDense, level, x_zero ? 1 : 0, L.x, L.b, L.t, nullptr);
+    std::swap(L.x, L.t);
+    return;
+  }
+  const int axis = L.line_mask == 1 ? 0 : (L.line_mask == 2 ? 1 : 2);
+  const auto sweeps = [&](int count, bool reverse) {
+    const int first = reverse ? 1 : 0;
+    for (int s = 0; s < count; ++s)
+      for (int pass = 0; pass < 2; ++pass)
+        add(kTailPcr, level, (first + pass) & 1, L.x, L.b, L.lfac[axis], nullptr);
+  };
+  DeviceLevel<T>& C = levels[level + 1];
+  sweeps(policy_.pre_sweeps, false);
+  add(kTailRestrict, level, L.coarsen_mask, L.x, L.b, C.b, C.x);
+  tail_cycle(levels, level + 1, counter, true, prog);
+  if (counter > 1) tail_cycle(levels, level + 1, counter - 1, false, prog);
+  add(kTailProlong, level, L.coarsen_mask, L.x, C.x, nullptr, nullptr);
+  sweeps(policy_.post_sweeps, true);
+}
+
+template <class T>
+void Solver::tail_launch(std::vector<DeviceLevel<T>>& levels, TailProgram<T>& prog) {
+  const int slot = std::is_same<T, float>::value ? 1 : 0;
+  const int count = static_cast<int>(levels.size()) - tail_level_;
+  for (int l = 0; l < count; ++l) {
+    const DeviceLevel<T>& L = levels[tail_level_ + l];
+    prog.levels[l] = L.view(neumann_);
+    prog.axis[l] = L.line_mask == 1 ? 0 : (L.line_mask == 2 ? 1 : 2);
+  }
+  prog.dense_op = coarse_op_;
+  prog.dense_n = levels.back().cells();
+  prog.scalars = d_scalars_;
+  launch_tail<T>(stream_, prog, tail_steps_, tail_blocks_[slot]);
+  launches_ += 1;
+}
+
 template <class T>
 void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter,
                    bool x_zero) {
@@ -795,8 +906,32 @@ void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter,
   // Retained defect + restrict_residual in one pass.
   launch_defect_restrict<T>(stream_, F.view(neumann_), F.x, F.b, C.view(neumann_),
                             C.b, C.x, F.coarsen_mask, F.split, C.split);
-  cycle(levels, level + 1, counter, true);
-  if (counter > 1) cycle(levels, level + 1, counter - 1, false);
+  if (level + 1 == tail_level_) {
+    // Both visits of the level below (an F-cycle's counter 2 and 1) in one
+    // persistent launch.
+    TailProgram<T> prog;
+    prog.count = 0;
+    std::vector<std::pair<T*, T*>> saved;
+    for (auto& L : levels) saved.emplace_back(L.x, L.t);
+    tail_cycle(levels, level + 1, counter, true, prog);
+    if (counter > 1) tail_cycle(levels, level + 1, counter - 1, false, prog);
+    if (prog.count <= kTailMaxOps) {
+      tail_launch(levels, prog);
+    } else {
+      for (size_t l = 0; l < levels.size(); ++l) {
+        levels[l].x = saved[l].first;
+        levels[l].t = saved[l].second;
+      }
+      const int tail = tail_level_;
+      tail_level_ = -1;
+      cycle(levels, level + 1, counter, true);
+      if (counter > 1) cycle(levels, level + 1, counter - 1, false);
+      tail_level_ = tail;
+    }
+  } else {
+    cycle(levels, level + 1, counter, true);
+    if (counter > 1) cycle(levels, level + 1, counter - 1, false);
+  }
   launch_prolongate<T>(stream_, F.view(neumann_), F.x, C.view(neumann_), C.x,
                        F.coarsen_mask, F.split, C.split);
   smooth(levels, level, policy_.post_sweeps, true, false);
@@ -918,7 +1053,12 @@ Status Solver::sync_scalars() {
                                     cudaMemcpyDeviceToHost, stream_),
                     "scalar readback");
   if (!st) return st;
-  return check(cudaStreamSynchronize(stream_), "solver step");
+  st = check(cudaStreamSynchronize(stream_), "solver step");
+  if (!st) return st;
+  if (h_scalars_->flags & 8)
+    return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric,
+                "small-level kernel: a grid barrier timed out");
+  return {};
 }
 
 // solve_pcg (src/solver_krylov.cpp:1299-1555) with identical control flow:
@@ -986,14 +1126,45 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
   st = restart_direction();
   if (!st) return st;
   uint32_t it = 0;
+  // Queue-ahead: in an iteration that is not a planned true-residual check,
+  // while the last recursive residual is far above the limit, the next MG
+  // application and direction update are queued before the host reads this
+  // iteration's scalars.  They are what the iteration does next unless its
+  // recursive residual has met the limit, and the true-residual check that
+  // then follows overwrites z, p and r.z anyway; so results are unchanged
+  // and the GPU does not idle while the host reads the scalars.
+  constexpr double kQueueAheadMargin = 8.0;
+  double last_recursive = result.initial_true_residual;
   while (it < control.maximum_iterations) {
     launch_spmv_dot(stream_, A, kp_, kap_, red(kOpPap));
     ++result.operator_applies;
     launch_pcg_update(stream_, n, kx_, kp_, kr_, kap_, red(kOpRecursive));
     launches_ += 2;
     ++it;
-    st = sync_scalars();
+    const bool planned = it % control.true_residual_interval == 0 ||
+                         it == control.maximum_iterations;
+    const bool ahead = queue_ahead_ && !planned && last_recursive > kQueueAheadMargin * tol;
+    st = check(cudaMemcpyAsync(h_scalars_, d_scalars_, sizeof(Scalars), cudaMemcpyDeviceToHost,
+                               stream_),
+               "scalar readback");
     if (!st) return st;
+    st = check(cudaEventRecord(scalars_ready_, stream_), "scalar event");
+    if (!st) return st;
+    if (ahead) {
+      st = precondition(mixed);
+      if (!st) return st;
+      if (!fused_dot) {
+        launch_dot(stream_, n, kr_, kz_, red(kOpRhoNext));
+        launches_ += 1;
+      }
+      launch_p_update(stream_, n, kp_, kz_, d_scalars_);
+      launches_ += 1;
+    }
+    st = check(cudaEventSynchronize(scalars_ready_), "solver step");
+    if (!st) return st;
+    if (h_scalars_->flags & 8)
+      return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric,
+                  "small-level kernel: a grid barrier timed out");
     result.iterations = it;
     // A breakdown flag comes from p.Ap of this iteration (the reference
     // stops before counting it) or from the r.z that formed this direction
@@ -1010,13 +1181,12 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
     }
     const double recursive = std::sqrt(h_scalars_->rr);
     result.recursive_residual = recursive;
+    last_recursive = recursive;
     if (history != nullptr && it - 1 < capacity) {
       history[it - 1] = recursive;
       result.history_length = it;
     }
-    const bool verify = recursive <= tol ||
-                        it % control.true_residual_interval == 0 ||
-                        it == control.maximum_iterations;
+    const bool verify = recursive <= tol || planned;
     if (verify) {
       launch_residual_norm(stream_, A, kx_, kb_, kr_, red(kOpRecursive));
       launches_ += 1;
@@ -1034,9 +1204,10 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
       if (!st) return st;
       continue;
     }
+    ++result.preconditioner_applies;
+    if (ahead) continue;  // already queued
     st = precondition(mixed);
     if (!st) return st;
-    ++result.preconditioner_applies;
     if (!fused_dot) {
       launch_dot(stream_, n, kr_, kz_, red(kOpRhoNext));
       launches_ += 1;
@@ -1852,7 +2023,7 @@ Status Solver::apply_preconditioner(const double* r, double* z, int memory,
   if (!st) return st;
   st = copy_out(z, kz_, n, memory);
   if (!st) return st;
-  return check(cudaStreamSynchronize(stream_), "preconditioner");
+  return sync_scalars();
 }
 
 Status Solver::adjoint(const double* solution, const double* dl_dp,
@@ -1986,6 +2157,10 @@ Status Solver::profile_kernel(int kernel, int repetitions, double* ms,
       case HFPS_KERNEL_PCG_UPDATE:
         launch_pcg_update(stream_, n, kx_, kp_, kr_, kap_, red(kOpMisc));
         per_cell = 48.0;
+        break;
+      case HFPS_KERNEL_RESIDUAL:
+        launch_residual_norm(stream_, A, kp_, kb_, kr_, red(kOpMisc));
+        per_cell = 56.0;
         break;
       case HFPS_KERNEL_MG_FP64:
       case HFPS_KERNEL_MG_MIXED:

@@ -115,6 +115,15 @@ class Solver {
               bool reverse, bool x_zero);
   template <class T>
   void coarse_solve(std::vector<DeviceLevel<T>>& levels, bool x_zero);
+  // The small levels as one persistent launch: tail_cycle appends the
+  // phases of cycle(level, counter) to `prog` exactly as cycle() would
+  // launch them (same buffer roles and swaps); tail_launch runs a program.
+  void select_tail();
+  template <class T>
+  void tail_cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter, bool x_zero,
+                  TailProgram<T>& prog);
+  template <class T>
+  void tail_launch(std::vector<DeviceLevel<T>>& levels, TailProgram<T>& prog);
   Status krylov_pcg(const hfps_control& control, hfps_result& result,
                     double* history, uint32_t capacity);
   Status krylov_fgmres(const hfps_control& control, hfps_result& result,
@@ -155,6 +164,8 @@ class Solver {
   double* kap_{};
   double* kb_{};
   bool krylov_fusion_{true};  // PCG's r.z formed in the MG exit
+  bool queue_ahead_{true};    // PCG queues the next MG before reading scalars
+  cudaEvent_t scalars_ready_{};  // the scalar readback of the current step
   Scalars* d_scalars_{};
   Scalars* h_scalars_{};      // pinned
   double* d_partials_{};
@@ -172,6 +183,11 @@ class Solver {
   double* coarse_op_{};
   int coarse_axis_{-1};
   bool coarse_dense_{};
+  // First level of the persistent small-level launch (-1: every phase is
+  // its own kernel), its PCR width and co-resident grid per precision.
+  int tail_level_{-1};
+  int tail_steps_{-1};
+  int tail_blocks_[2]{};
   // FGMRES basis: V_0..V_restart, Z_0..Z_{restart-1} and the operator image,
   // allocated on first use for the largest restart asked for.
   double* fg_storage_{};
