@@ -62,6 +62,12 @@ def parse():
     p.add_argument("--single", choices=["fp64", "mixed", "fgmres", "fgmres-mixed"], default=None,
                    help="profiling aid: one warm-up solve, then one solve, no timing/JSON "
                         "(PCG, or the production FGMRES(12) with the residual-minimising MG)")
+    p.add_argument("--kernel", choices=["operator", "smooth_fp64", "smooth_fp32", "restrict_fp64",
+                                        "prolong_fp64", "pcg_update", "mg_fp64", "mg_mixed",
+                                        "residual"],
+                   default=None,
+                   help="profiling aid: time `--steps` launches of one level-0 kernel class "
+                        "(or one MG application) with CUDA events; one JSON line, not the bench")
     p.add_argument("--config", choices=["three_spheres512"], default=None,
                    help="the 512^3 three-sphere mixed forward + adjoint sequence "
                         "(its own JSON line; not the headline metric)")
@@ -592,6 +598,20 @@ def run_single(args):
     solver.close()
 
 
+def run_kernel(args):
+    """`steps` launches of one kernel class on the solver's stream (after
+    hfps_profile_kernel's own warm-up launch), timed with CUDA events."""
+    import hfps
+    system = make_system(args)
+    solver = hfps.PressureSolver.from_system(system, hfps.Policy.production())
+    ms, nbytes = solver.profile_kernel(args.kernel, args.steps)
+    print(json.dumps({"kernel": args.kernel, "shape": list(system.rhs.shape[::-1]),
+                      "launches": args.steps, "ms_per_launch": ms,
+                      "algorithmic_bytes": nbytes,
+                      "gb_s": nbytes / (ms * 1e-3) / 1e9 if nbytes > 0 else None}))
+    solver.close()
+
+
 def run_three_spheres(args):
     """512^3 spherical flame with three IBM spheres: `steps` warm-started
     mixed-precision forward solves, each followed by a mixed adjoint solve of
@@ -681,6 +701,9 @@ def main():
     world, rank, local = dist_setup(args)
     if args.single:
         run_single(args)
+        return
+    if args.kernel:
+        run_kernel(args)
         return
     if args.config == "three_spheres512":
         run_three_spheres(args)

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 
 namespace hfps {
 namespace {
@@ -339,6 +340,20 @@ __global__ void __launch_bounds__(kRowThreads)
       v[a][b] = __ldg(cx + cpos(xp + C.nx * (j + C.ny * zq), xp, j, zq));
     }
   }
+  // The four fine values and flags are loaded before any store: a load
+  // issued after a store to the same array cannot be hoisted above it, and
+  // would otherwise wait on the previous cell's load.
+  T old[2][2];
+  bool fluid[2][2];
+#pragma unroll
+  for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx) {
+      const int i = 2 * p + dx, k = 2 * q + dz;
+      const bool in = i < F.nx && k < F.nz;
+      fluid[dz][dx] = in && F.fluid[i + F.nx * (j + F.ny * k)] != 0;
+      old[dz][dx] = in ? x[2 * hx * (j + F.ny * k) + dx * hx + p] : T(0);
+    }
 #pragma unroll
   for (int dz = 0; dz < 2; ++dz) {
     const int k = 2 * q + dz;
@@ -355,10 +370,7 @@ __global__ void __launch_bounds__(kRowThreads)
       double xw;
       interp_axis(i, 1, C.nx, xl, xr, xw);
       const bool two_x = xl != xr;
-      const int c = i + F.nx * (j + F.ny * k);
       const int at = 2 * hx * (j + F.ny * k) + dx * hx + p;
-      const bool fluid = F.fluid[c] != 0;
-      const T old = x[at];
       T value = T(0);
 #pragma unroll
       for (int az = 0; az < 2; ++az)
@@ -373,7 +385,7 @@ __global__ void __launch_bounds__(kRowThreads)
           const T sum = value + term;
           value = on ? sum : value;
         }
-      x[at] = fluid ? old + value : T(0);
+      x[at] = fluid[dz][dx] ? old[dz][dx] + value : T(0);
     }
   }
 }
@@ -543,6 +555,97 @@ __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
   });
   if (finish_reduction<1>(v, red) && threadIdx.x == 0)
     apply_scalar_op(red.scalars, red.op, v[0]);
+}
+
+// The same two Krylov stencil kernels over 3-D tiles: a CTA of kTileX x
+// kTileY threads owns those columns of (i, j) and marches up kTileZ planes.
+// Each plane of x is read from HBM once: the thread keeps its column's
+// x(k-1), x(k), x(k+1) in registers and publishes x(k) in a shared-memory
+// tile with a one-cell ring, from which the four in-plane neighbours are
+// read; the z-faces' upper value is carried to the next plane.  The row is
+// evaluated as row_value evaluates it (same terms, same order), so y is
+// bit-identical to the row-walking kernels; the reduction groups its
+// partial sums by tile.
+constexpr int kTileX = 32;
+constexpr int kTileY = 8;
+constexpr int kTileZ = 32;
+// Tiles per launch: at most one reduction partial each in the solver's
+// partials block (kBasisChunk * 148 * 8 doubles and more).
+constexpr long long kMaxTiledBlocks = 16384;
+
+template <int MODE>  // 0: y = A x and x.y; 1: r = b - A x and r.r
+__global__ void __launch_bounds__(kTileX * kTileY)
+    k_stencil_tiled(Level<double> L, const double* __restrict__ x, const double* __restrict__ b,
+                    double* __restrict__ y, Reduce red) {
+  grid_dependency_sync();
+  __shared__ double tile[2][kTileY + 2][kTileX + 2];
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  const int tiles_x = (nx + kTileX - 1) / kTileX;
+  const int tiles_y = (ny + kTileY - 1) / kTileY;
+  const int bx = blockIdx.x % tiles_x;
+  const int rest = blockIdx.x / tiles_x;
+  const int by = rest % tiles_y;
+  const int bz = rest / tiles_y;
+  const int tx = threadIdx.x % kTileX, ty = threadIdx.x / kTileX;
+  const int i = bx * kTileX + tx, j = by * kTileY + ty;
+  const int k0 = bz * kTileZ, k1 = min(nz, k0 + kTileZ);
+  const bool on = i < nx && j < ny;
+  const int ic = min(i, nx - 1), jc = min(j, ny - 1);
+  const int plane = nx * ny;
+  const unsigned nb = L.neumann;
+  // Ring loads of this thread (in-plane neighbours outside the tile).
+  const bool ring_w = tx == 0 && i > 0 && on;
+  const bool ring_e = (tx == kTileX - 1 || i == nx - 1) && i + 1 < nx && on;
+  const bool ring_s = ty == 0 && j > 0 && on;
+  const bool ring_n = (ty == kTileY - 1 || j == ny - 1) && j + 1 < ny && on;
+  int c = ic + nx * (jc + ny * k0);
+  double x_prev = (on && k0 > 0) ? x[c - plane] : 0.0;
+  double x_cur = on ? x[c] : 0.0;
+  double fz_lo = on ? L.fz[c] : 0.0;
+  double acc[1] = {0.0};
+  int buf = 0;
+  for (int k = k0; k < k1; ++k, c += plane) {
+    const double x_next = (on && k + 1 < nz) ? x[c + plane] : 0.0;
+    tile[buf][ty + 1][tx + 1] = x_cur;
+    if (ring_w) tile[buf][ty + 1][tx] = x[c - 1];
+    if (ring_e) tile[buf][ty + 1][tx + 2] = x[c + 1];
+    if (ring_s) tile[buf][ty][tx + 1] = x[c - nx];
+    if (ring_n) tile[buf][ty + 2][tx + 1] = x[c + nx];
+    __syncthreads();
+    if (on) {
+      const double xc = x_cur;
+      const double xm = i > 0 ? tile[buf][ty + 1][tx] : ((nb & 1u) ? xc : 0.0);
+      const double xp = i + 1 < nx ? tile[buf][ty + 1][tx + 2] : ((nb & 2u) ? xc : 0.0);
+      const double ym = j > 0 ? tile[buf][ty][tx + 1] : ((nb & 4u) ? xc : 0.0);
+      const double yp = j + 1 < ny ? tile[buf][ty + 2][tx + 1] : ((nb & 8u) ? xc : 0.0);
+      const double zm = k > 0 ? x_prev : ((nb & 16u) ? xc : 0.0);
+      const double zp = k + 1 < nz ? x_next : ((nb & 32u) ? xc : 0.0);
+      const int fxi = face_x_index(L, c, j, k);
+      const int fyi = face_y_index(L, c, k);
+      const double fz_hi = L.fz[c + plane];
+      double v = L.diag[c] * xc;
+      v -= L.fx[fxi] * xm;
+      v -= L.fx[fxi + 1] * xp;
+      v -= L.fy[fyi] * ym;
+      v -= L.fy[fyi + nx] * yp;
+      v -= fz_lo * zm;
+      v -= fz_hi * zp;
+      if (MODE == 0) {
+        y[c] = v;
+        acc[0] += xc * v;
+      } else {
+        const double r = b[c] - v;
+        y[c] = r;
+        acc[0] += r * r;
+      }
+      fz_lo = fz_hi;
+    }
+    x_prev = x_cur;
+    x_cur = x_next;
+    buf ^= 1;
+  }
+  if (finish_reduction<1>(acc, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, acc[0]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1406,13 +1509,36 @@ void launch_mg_projection(cudaStream_t s, int n, const double* r,
                                                               recursive, red);
 }
 
+// The tiled stencil kernels serve grids whose tile count fits the reduction
+// partials; HFPS_TILED_STENCIL=0 keeps the row-walking kernels.
+bool use_tiled_stencil(const Level<double>& L) {
+  const char* env = std::getenv("HFPS_TILED_STENCIL");
+  const bool enabled = !(env != nullptr && env[0] == '0');
+  const long long tiles = static_cast<long long>((L.nx + kTileX - 1) / kTileX) *
+                          ((L.ny + kTileY - 1) / kTileY) * ((L.nz + kTileZ - 1) / kTileZ);
+  return enabled && tiles <= kMaxTiledBlocks;
+}
+int tiled_blocks(const Level<double>& L) {
+  return ((L.nx + kTileX - 1) / kTileX) * ((L.ny + kTileY - 1) / kTileY) *
+         ((L.nz + kTileZ - 1) / kTileZ);
+}
+
 void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
                      double* y, Reduce red) {
+  if (use_tiled_stencil(L)) {
+    launch(k_stencil_tiled<0>, tiled_blocks(L), kTileX * kTileY, 0, s, L, x,
+           static_cast<const double*>(nullptr), y, red);
+    return;
+  }
   launch(k_spmv_dot, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, x, y, red);
 }
 void launch_residual_norm(cudaStream_t s, const Level<double>& L,
                           const double* x, const double* b, double* r,
                           Reduce red) {
+  if (use_tiled_stencil(L)) {
+    launch(k_stencil_tiled<1>, tiled_blocks(L), kTileX * kTileY, 0, s, L, x, b, r, red);
+    return;
+  }
   launch(k_residual_norm, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, x, b, r,
                                                                        red);
 }

@@ -144,7 +144,7 @@ EXPORTS = ["hfps_default_policy", "hfps_production_policy", "hfps_default_contro
            "hfps_operator_dot_noalloc", "hfps_last_error", "hfps_destroy"]
 
 KERNELS = {"operator": 0, "smooth_fp64": 1, "smooth_fp32": 2, "restrict_fp64": 3,
-           "prolong_fp64": 4, "pcg_update": 5, "mg_fp64": 6, "mg_mixed": 7}
+           "prolong_fp64": 4, "pcg_update": 5, "mg_fp64": 6, "mg_mixed": 7, "residual": 8}
 
 
 def _lib():

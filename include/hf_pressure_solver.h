@@ -305,7 +305,8 @@ typedef enum hfps_kernel {
   HFPS_KERNEL_PROLONG_FP64 = 4,    /* level-1 -> level-0 prolongation */
   HFPS_KERNEL_PCG_UPDATE = 5,      /* x += a p, r -= a Ap, |r|^2 */
   HFPS_KERNEL_MG_FP64 = 6,         /* one whole FP64 MG application */
-  HFPS_KERNEL_MG_MIXED = 7         /* one whole FP32 MG application */
+  HFPS_KERNEL_MG_MIXED = 7,        /* one whole FP32 MG application */
+  HFPS_KERNEL_RESIDUAL = 8         /* level-0 true residual r = b - A x with |r|^2 */
 } hfps_kernel;
 
 /* Launches one kernel class `repetitions` times on the solver's stream
