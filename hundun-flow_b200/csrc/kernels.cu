@@ -557,15 +557,16 @@ __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
     apply_scalar_op(red.scalars, red.op, v[0]);
 }
 
-// The same two Krylov stencil kernels over 3-D tiles: a CTA of kTileX x
+// The Krylov operator y = A x with x.y over 3-D tiles: a CTA of kTileX x
 // kTileY threads owns those columns of (i, j) and marches up kTileZ planes.
 // Each plane of x is read from HBM once: the thread keeps its column's
 // x(k-1), x(k), x(k+1) in registers and publishes x(k) in a shared-memory
 // tile with a one-cell ring, from which the four in-plane neighbours are
 // read; the z-faces' upper value is carried to the next plane.  The row is
 // evaluated as row_value evaluates it (same terms, same order), so y is
-// bit-identical to the row-walking kernels; the reduction groups its
-// partial sums by tile.
+// bit-identical to k_spmv_dot's; the reduction groups its partial sums by
+// tile.  (The same tiling for the true residual r = b - A x was slower than
+// k_residual_norm at 256^3, 0.208 against 0.180 ms, and is not used.)
 constexpr int kTileX = 32;
 constexpr int kTileY = 8;
 constexpr int kTileZ = 32;
@@ -573,10 +574,9 @@ constexpr int kTileZ = 32;
 // partials block (kBasisChunk * 148 * 8 doubles and more).
 constexpr long long kMaxTiledBlocks = 16384;
 
-template <int MODE>  // 0: y = A x and x.y; 1: r = b - A x and r.r
 __global__ void __launch_bounds__(kTileX * kTileY)
-    k_stencil_tiled(Level<double> L, const double* __restrict__ x, const double* __restrict__ b,
-                    double* __restrict__ y, Reduce red) {
+    k_stencil_tiled(Level<double> L, const double* __restrict__ x, double* __restrict__ y,
+                    Reduce red) {
   grid_dependency_sync();
   __shared__ double tile[2][kTileY + 2][kTileX + 2];
   const int nx = L.nx, ny = L.ny, nz = L.nz;
@@ -630,14 +630,8 @@ __global__ void __launch_bounds__(kTileX * kTileY)
       v -= L.fy[fyi + nx] * yp;
       v -= fz_lo * zm;
       v -= fz_hi * zp;
-      if (MODE == 0) {
-        y[c] = v;
-        acc[0] += xc * v;
-      } else {
-        const double r = b[c] - v;
-        y[c] = r;
-        acc[0] += r * r;
-      }
+      y[c] = v;
+      acc[0] += xc * v;
       fz_lo = fz_hi;
     }
     x_prev = x_cur;
@@ -1509,8 +1503,8 @@ void launch_mg_projection(cudaStream_t s, int n, const double* r,
                                                               recursive, red);
 }
 
-// The tiled stencil kernels serve grids whose tile count fits the reduction
-// partials; HFPS_TILED_STENCIL=0 keeps the row-walking kernels.
+// The tiled operator serves grids whose tile count fits the reduction
+// partials; HFPS_TILED_STENCIL=0 keeps the row-walking kernel.
 bool use_tiled_stencil(const Level<double>& L) {
   const char* env = std::getenv("HFPS_TILED_STENCIL");
   const bool enabled = !(env != nullptr && env[0] == '0');
@@ -1526,8 +1520,7 @@ int tiled_blocks(const Level<double>& L) {
 void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
                      double* y, Reduce red) {
   if (use_tiled_stencil(L)) {
-    launch(k_stencil_tiled<0>, tiled_blocks(L), kTileX * kTileY, 0, s, L, x,
-           static_cast<const double*>(nullptr), y, red);
+    launch(k_stencil_tiled, tiled_blocks(L), kTileX * kTileY, 0, s, L, x, y, red);
     return;
   }
   launch(k_spmv_dot, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, x, y, red);
@@ -1535,10 +1528,6 @@ void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
 void launch_residual_norm(cudaStream_t s, const Level<double>& L,
                           const double* x, const double* b, double* r,
                           Reduce red) {
-  if (use_tiled_stencil(L)) {
-    launch(k_stencil_tiled<1>, tiled_blocks(L), kTileX * kTileY, 0, s, L, x, b, r, red);
-    return;
-  }
   launch(k_residual_norm, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, x, b, r,
                                                                        red);
 }

@@ -31,14 +31,11 @@ struct Scalars {
                      // bit 3 a grid barrier of the small-level kernel timed out
   unsigned marks;    // bit 0: a difference had a nonzero entry (recycle capture)
   unsigned counters[8];  // last-block arrival counters, one per reduction
-  // The small-level kernel's grid barrier: arrivals and completed barriers,
-  // 128 bytes apart so that polling the one does not slow the atomics on the
-  // other.
+  // The small-level kernel's grid barrier: arrivals (on a 128-byte line of
+  // its own).
   unsigned tail_pad0[32];
   unsigned tail_count;
   unsigned tail_pad1[31];
-  unsigned tail_generation;
-  unsigned tail_pad2[31];
 };
 
 enum ScalarOp : int {

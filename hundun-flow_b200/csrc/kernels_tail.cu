@@ -25,42 +25,38 @@
 namespace hfps {
 namespace {
 
-constexpr long long kTailSpinLimit = 1LL << 24;  // polls of ~64 ns: about a second
+constexpr long long kTailSpinLimit = 1LL << 23;  // polls of an L2 round trip: about 4 s
 
 // Grid-wide barrier over `blocks` co-resident CTAs (cooperative launch).
-// Arrival publishes this CTA's writes (release); leaving after the
-// generation flips makes every other CTA's writes visible (acquire).
+// tail_count only grows, by one per CTA per barrier, so it is a multiple of
+// `blocks` between barriers (the solver clears it at the start of every
+// solve); a CTA's arrival ticket gives the count that ends its barrier.  The
+// arrival is acquire-release: it publishes this CTA's writes, and leaving
+// once the count is reached makes every other CTA's writes visible.
 __device__ __forceinline__ bool tail_barrier(Scalars* sc, unsigned blocks) {
   __shared__ int failed;
   __syncthreads();
   if (threadIdx.x == 0) {
     int bad = 0;
-    unsigned gen;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(gen) : "l"(&sc->tail_generation)
-                 : "memory");
+    unsigned ticket;
     __threadfence();
-    const unsigned arrived = atomicAdd(&sc->tail_count, 1u);
-    if (arrived == blocks - 1) {
-      atomicExch(&sc->tail_count, 0u);
-      __threadfence();
-      atomicAdd(&sc->tail_generation, 1u);
-    } else {
-      long long polls = 0;
-      while (true) {
-        unsigned now;
-        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now)
-                     : "l"(&sc->tail_generation) : "memory");
-        if (now != gen) break;
-        if (++polls > kTailSpinLimit) {
-          atomicOr(&sc->flags, 8);
-          bad = 1;
-          break;
-        }
-        __nanosleep(32);
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(ticket)
+                 : "l"(&sc->tail_count) : "memory");
+    const unsigned target = (ticket / blocks + 1) * blocks;
+    long long polls = 0;
+    while (true) {
+      unsigned now;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(now) : "l"(&sc->tail_count)
+                   : "memory");
+      if (static_cast<int>(now - target) >= 0) break;
+      if (++polls > kTailSpinLimit) {
+        atomicOr(&sc->flags, 8);
+        bad = 1;
+        break;
       }
     }
     int flags;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(flags) : "l"(&sc->flags)
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(flags) : "l"(&sc->flags)
                  : "memory");
     failed = bad || (flags & 8) != 0;
     __threadfence();

@@ -796,7 +796,8 @@ void Solver::coarse_solve(std::vector<DeviceLevel<T>>& levels, bool x_zero) {
 // non-coarsest one relaxes lines along one axis with PCR (few lines per
 // colour), all have the same line length, and the coarsest is the dense
 // affine map.  HFPS_TAIL=1 / 0 turns it on / off (default kTailDefault);
-// HFPS_TAIL_BLOCKS overrides its CTA count (clamped to what is co-resident).
+// HFPS_TAIL_BLOCKS overrides its CTA count (clamped to what is co-resident
+// and rounded down to a power of two).
 void Solver::select_tail() {
   tail_level_ = -1;
   const char* env = std::getenv("HFPS_TAIL");
@@ -834,9 +835,13 @@ void Solver::select_tail() {
   int want = std::max((lines + per_cta - 1) / per_cta, (dense_n + 31) / 32);
   const char* blocks_env = std::getenv("HFPS_TAIL_BLOCKS");
   if (blocks_env != nullptr && std::atoi(blocks_env) > 0) want = std::atoi(blocks_env);
-  tail_blocks_[0] = std::min(tail_grid<double>(steps, dense_n, sms), want);
-  tail_blocks_[1] = std::min(tail_grid<float>(steps, dense_n, sms), want);
-  if (tail_blocks_[0] < 1 || tail_blocks_[1] < 1) return;
+  // One CTA count for both precisions, a power of two: the barrier's
+  // arrival counter is then a multiple of it across 32-bit wrap-around.
+  int blocks = std::min({tail_grid<double>(steps, dense_n, sms),
+                         tail_grid<float>(steps, dense_n, sms), want});
+  if (blocks < 1) return;
+  while (blocks & (blocks - 1)) blocks &= blocks - 1;
+  tail_blocks_[0] = tail_blocks_[1] = blocks;
   tail_level_ = first;
   tail_steps_ = steps;
 }

@@ -1,9 +1,9 @@
-"""The Krylov stencil kernels over 3-D tiles (k_stencil_tiled: A p with p.Ap,
-r = b - A x with r.r) against the row-walking kernels (HFPS_TILED_STENCIL=0,
-read at every launch).  Rows are evaluated in the same order, so only the
-grouping of the reduction partials differs: PCG and FGMRES solves take the
-same iteration count (+-1) and agree to 1e-10, on even and ragged extents
-(partial tiles in x, y and z), Dirichlet and Neumann faces."""
+"""The Krylov operator over 3-D tiles (k_stencil_tiled: A p with p.Ap)
+against the row-walking kernel (HFPS_TILED_STENCIL=0, read at every launch).
+Rows are evaluated in the same order, so only the grouping of the
+reduction partials differs: PCG and FGMRES solves take the same iteration
+count (+-1) and agree to 1e-10, on even and ragged extents (partial tiles in
+x, y and z), Dirichlet and Neumann faces."""
 import os
 
 import numpy as np
