@@ -589,11 +589,16 @@ struct ScanShape {
   int lpb, chunks, rows;
 };
 
+// Lines per block are halved (down to HFPS_SCAN_MIN_LPB) while a colour has
+// fewer than two blocks per SM.
+#ifndef HFPS_SCAN_MIN_LPB
+#define HFPS_SCAN_MIN_LPB 8
+#endif
 template <class T>
 ScanShape scan_shape(long long per_color, int extent) {
   constexpr int rows = ScanConfig<T>::rows;
   ScanShape sh{32, (extent + rows - 1) / rows, 0};
-  while (sh.lpb > 8 && per_color < 296LL * sh.lpb) sh.lpb >>= 1;
+  while (sh.lpb > HFPS_SCAN_MIN_LPB && per_color < 296LL * sh.lpb) sh.lpb >>= 1;
   while (sh.lpb > 1 && sh.lpb * sh.chunks > ScanConfig<T>::threads) sh.lpb >>= 1;
   sh.rows = (extent + sh.chunks - 1) / sh.chunks;
   return sh;
