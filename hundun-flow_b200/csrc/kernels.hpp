@@ -159,6 +159,10 @@ template <class T>
 struct TailProgram {
   int count;
   int dense_n;
+  // Added to every barrier's target count: 0, or 1 to make the first
+  // barrier run out its wait limit (the failure path's test).
+  int barrier_offset;
+  int pad;
   int axis[kTailMaxLevels];
   Level<T> levels[kTailMaxLevels];
   const double* dense_op;

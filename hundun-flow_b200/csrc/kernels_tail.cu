@@ -16,16 +16,18 @@
 // those of that path.
 //
 // The barrier is bounded: a CTA that waits longer than kTailSpinLimit polls
-// records the failure in the solver's scalars (flag bit 3) and the program
-// ends on every CTA, so a wait can never hang the GPU; the solver reports a
-// preconditioner failure at its next check.
+// (under a second) records the failure in the solver's scalars (flag bit 3)
+// and the program ends on every CTA, so a wait can never hang the GPU; the
+// solver reports a preconditioner failure at its next check.  A program with
+// barrier_offset 1 never reaches its first barrier's count, which is how the
+// tests exercise that path.
 #include "kernels.hpp"
 #include "phase_device.cuh"
 
 namespace hfps {
 namespace {
 
-constexpr long long kTailSpinLimit = 1LL << 23;  // polls of an L2 round trip: about 4 s
+constexpr long long kTailSpinLimit = 1LL << 21;  // polls of an L2 round trip: under a second
 
 // Grid-wide barrier over `blocks` co-resident CTAs (cooperative launch).
 // tail_count only grows, by one per CTA per barrier, so it is a multiple of
@@ -33,7 +35,7 @@ constexpr long long kTailSpinLimit = 1LL << 23;  // polls of an L2 round trip: a
 // solve); a CTA's arrival ticket gives the count that ends its barrier.  The
 // arrival is acquire-release: it publishes this CTA's writes, and leaving
 // once the count is reached makes every other CTA's writes visible.
-__device__ __forceinline__ bool tail_barrier(Scalars* sc, unsigned blocks) {
+__device__ __forceinline__ bool tail_barrier(Scalars* sc, unsigned blocks, unsigned offset) {
   __shared__ int failed;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -42,7 +44,7 @@ __device__ __forceinline__ bool tail_barrier(Scalars* sc, unsigned blocks) {
     __threadfence();
     asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(ticket)
                  : "l"(&sc->tail_count) : "memory");
-    const unsigned target = (ticket / blocks + 1) * blocks;
+    const unsigned target = (ticket / blocks + 1) * blocks + offset;
     long long polls = 0;
     while (true) {
       unsigned now;
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(kTailThreads, 1) k_tail(TailProgram<T> prog) {
       default:
         break;
     }
-    if (!tail_barrier(prog.scalars, blocks)) return;
+    if (!tail_barrier(prog.scalars, blocks, static_cast<unsigned>(prog.barrier_offset))) return;
   }
 }
 

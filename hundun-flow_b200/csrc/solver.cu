@@ -802,6 +802,11 @@ void Solver::select_tail() {
   tail_level_ = -1;
   const char* env = std::getenv("HFPS_TAIL");
   const bool on = env != nullptr && env[0] != '\0' ? env[0] != '0' : kTailDefault;
+  // HFPS_TAIL_BARRIER_TEST=1: every launch's first grid barrier runs out its
+  // wait limit, so the solve fails with the barrier's status (for the test of
+  // that path; the GPU stays usable).
+  const char* test = std::getenv("HFPS_TAIL_BARRIER_TEST");
+  tail_barrier_test_ = test != nullptr && test[0] == '1';
   if (!on || !coarse_dense_) return;
   const int levels = static_cast<int>(l64_.size());
   int first = levels - 1;
@@ -893,6 +898,8 @@ void Solver::tail_launch(std::vector<DeviceLevel<T>>& levels, TailProgram<T>& pr
   }
   prog.dense_op = coarse_op_;
   prog.dense_n = levels.back().cells();
+  prog.barrier_offset = tail_barrier_test_ ? 1 : 0;
+  prog.pad = 0;
   prog.scalars = d_scalars_;
   launch_tail<T>(stream_, prog, tail_steps_, tail_blocks_[slot]);
   launches_ += 1;

@@ -188,6 +188,7 @@ class Solver {
   int tail_level_{-1};
   int tail_steps_{-1};
   int tail_blocks_[2]{};
+  bool tail_barrier_test_{false};
   // FGMRES basis: V_0..V_restart, Z_0..Z_{restart-1} and the operator image,
   // allocated on first use for the largest restart asked for.
   double* fg_storage_{};

@@ -89,3 +89,37 @@ def test_tail_launch_matches_per_phase_kernels(hfps_mod, case, unit):
     assert b["kernel_launches"] < a["kernel_launches"]
     plain.close()
     tail.close()
+
+
+def test_barrier_timeout_reports_failure(hfps_mod):
+    """HFPS_TAIL_BARRIER_TEST=1 sets every launch's first barrier target one
+    arrival beyond the grid, so its bounded wait runs out (under a second):
+    the kernel records flag bit 3 and returns, and the solve fails with
+    numerical_failure naming the barrier.  The GPU stays usable: a solver
+    made afterwards in the same process solves normally."""
+    import time
+    s = CASES["y_lines_96x128x64"]()
+    policy = hfps_mod.Policy.production()
+    saved = os.environ.get("HFPS_TAIL_BARRIER_TEST")
+    os.environ["HFPS_TAIL_BARRIER_TEST"] = "1"
+    try:
+        stalled = make_solver(hfps_mod, s, policy, tail=True)
+    finally:
+        if saved is None:
+            os.environ.pop("HFPS_TAIL_BARRIER_TEST", None)
+        else:
+            os.environ["HFPS_TAIL_BARRIER_TEST"] = saved
+    t0 = time.perf_counter()
+    with pytest.raises(hfps_mod.SolverError) as err:
+        stalled.solve(s.rhs, rtol=1e-10, maxit=50)
+    assert time.perf_counter() - t0 < 60.0
+    assert "grid barrier timed out" in str(err.value)
+    stalled.close()
+    fresh = make_solver(hfps_mod, s, policy, tail=True)
+    x, info = fresh.solve(s.rhs, rtol=1e-10, maxit=400)
+    assert info["termination"] == "converged"
+    plain = make_solver(hfps_mod, s, policy, tail=False)
+    y, _ = plain.solve(s.rhs, rtol=1e-10, maxit=400)
+    assert np.array_equal(x, y)
+    fresh.close()
+    plain.close()
