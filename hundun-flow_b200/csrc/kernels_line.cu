@@ -198,12 +198,16 @@ struct ScanConfig<double> {
   static constexpr bool symmetric = true;
   static constexpr int arrays = 2;
 };
+// FP32 factors in the symmetric two-array form when HFPS_SCAN_SYM_F32 is 1.
+#ifndef HFPS_SCAN_SYM_F32
+#define HFPS_SCAN_SYM_F32 0
+#endif
 template <>
 struct ScanConfig<float> {
   static constexpr int rows = HFPS_SCAN_ROWS_F32;
   static constexpr int threads = HFPS_SCAN_THREADS_F32;
-  static constexpr bool symmetric = false;
-  static constexpr int arrays = 3;
+  static constexpr bool symmetric = HFPS_SCAN_SYM_F32 != 0;
+  static constexpr int arrays = symmetric ? 2 : 3;
 };
 // Longest line both precisions can solve: every chunk of a line lives in
 // one block.
