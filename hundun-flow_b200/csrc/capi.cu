@@ -80,6 +80,7 @@ void hfps_default_control(hfps_control* c) {
   c->algorithm = HFPS_PCG;
   c->precision = HFPS_FP64;
   c->recycle = HFPS_RECYCLE_NONE;
+  c->norm = HFPS_NORM_PLAIN;
 }
 
 int hfps_create(const hfps_geometry* geometry, const hfps_policy* policy,

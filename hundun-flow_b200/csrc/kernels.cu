@@ -98,11 +98,58 @@ __device__ void apply_scalar_op(Scalars* sc, int op, double sum) {
       sc->rho = sum;
       sc->beta = 0.0;
       break;
+    case kOpScaledNorm: {
+      const double scale = sc->misc[2];
+      const double norm = scale == 0.0 ? 0.0 : scale * sqrt(sum);
+      sc->misc[3] = norm;
+      if (!(sum >= 0.0) || !isfinite(norm)) sc->flags |= 1;
+      break;
+    }
     default:
       sc->misc[0] = sum;
       if (!isfinite(sum)) sc->flags |= 1;
       break;
   }
+}
+
+// Grid-wide maximum of non-negative values, in finish_reduction's pattern:
+// each block's maximum goes to the partials, and the last block to arrive
+// (counter `counter`) takes their maximum.  Maxima do not depend on the
+// order, so the result is exact and reproducible.  Returns true in the last
+// block, whose thread 0 then holds the result in v.
+__device__ double block_max(double v) {
+  __shared__ double warp_max[32];
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) warp_max[warp] = v;
+  __syncthreads();
+  double m = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < static_cast<int>((blockDim.x + 31) >> 5); ++w) m = fmax(m, warp_max[w]);
+  return m;
+}
+
+__device__ bool finish_max(double& v, Scalars* sc, double* partials, int counter) {
+  const double m = block_max(v);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = m;
+    __threadfence();
+    last = atomicAdd(&sc->counters[counter], 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return false;
+  __threadfence();
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < static_cast<int>(gridDim.x); b += blockDim.x)
+    acc = fmax(acc, reinterpret_cast<volatile double*>(partials)[b]);
+  acc = block_max(acc);
+  if (threadIdx.x == 0) {
+    v = acc;
+    sc->counters[counter] = 0u;
+  }
+  return true;
 }
 
 // Index of natural cell c in a vector of layout v.
@@ -916,6 +963,41 @@ __global__ void k_norm2(int n, const double* __restrict__ a, Reduce red) {
     apply_scalar_op(red.scalars, red.op, v[0]);
 }
 
+// The two passes of the max-scaled norm (global_norm, src/solver_krylov.cpp:
+// 650-711): max |v| into misc[2], a non-finite entry setting flag bit 0;
+// then the sum of (v / max)^2, which kOpScaledNorm turns into
+// misc[3] = max * sqrt(sum).  The reference sums each rank's squares with
+// Neumaier compensation; here the sum is the fixed-order FP64 tree.
+__global__ void k_norm_max(int n, const double* __restrict__ a, Scalars* sc,
+                           double* partials) {
+  grid_dependency_sync();
+  double m = 0.0;
+  bool bad = false;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const double value = a[c];
+    if (!isfinite(value)) bad = true;
+    else m = fmax(m, fabs(value));
+  }
+  if (bad) atomicOr(&sc->flags, 1);
+  if (finish_max(m, sc, partials, kOpScaledNorm) && threadIdx.x == 0) sc->misc[2] = m;
+}
+
+__global__ void k_norm_scaled_sum(int n, const double* __restrict__ a, Reduce red) {
+  grid_dependency_sync();
+  const double scale = red.scalars->misc[2];
+  double v[1] = {0.0};
+  if (scale > 0.0) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+         c += gridDim.x * blockDim.x) {
+      const double scaled = a[c] / scale;
+      v[0] += scaled * scaled;
+    }
+  }
+  if (finish_reduction<1>(v, red) && threadIdx.x == 0)
+    apply_scalar_op(red.scalars, red.op, v[0]);
+}
+
 __global__ void k_p_update(int n, double* __restrict__ p,
                            const double* __restrict__ z,
                            const Scalars* __restrict__ sc) {
@@ -1541,6 +1623,12 @@ void launch_dot(cudaStream_t s, int n, const double* a, const double* b,
 }
 void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red) {
   launch(k_norm2, reduction_blocks(n), kThreads, 0, s, n, v, red);
+}
+void launch_scaled_norm(cudaStream_t s, int n, const double* v, Scalars* scalars,
+                        double* partials) {
+  launch(k_norm_max, reduction_blocks(n), kThreads, 0, s, n, v, scalars, partials);
+  launch(k_norm_scaled_sum, reduction_blocks(n), kThreads, 0, s, n, v,
+         Reduce{scalars, partials, kOpScaledNorm});
 }
 void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc) {

@@ -44,9 +44,10 @@ enum ScalarOp : int {
   kOpRhoNext = 2,    // rho_next = sum; beta = rho_next / rho; rho = rho_next
   kOpRhoRestart = 3, // rho = sum; beta = 0
   kOpMisc = 4,       // misc[0] = sum
+  kOpScaledNorm = 7, // misc[3] = misc[2] * sqrt(sum): the max-scaled norm (counter 7)
 };
 // Arrival counters of reductions that apply no scalar op: 5 MG projection,
-// 6 FGMRES multidot.
+// 6 FGMRES multidot.  Counter 7 serves both passes of the max-scaled norm.
 constexpr int kCounterProjection = 5;
 constexpr int kCounterMultidot = 6;
 constexpr int kMaxFgmresRestart = 64;
@@ -216,6 +217,11 @@ void launch_dot(cudaStream_t s, int n, const double* a, const double* b,
 void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc);
 void launch_norm2(cudaStream_t s, int n, const double* v, Reduce red);
+// The max-scaled 2-norm of global_norm (src/solver_krylov.cpp:650-711) into
+// scalars->misc[3]: pass 1 forms max |v| (misc[2]; a non-finite entry sets
+// flag bit 0), pass 2 max * sqrt(sum of (v / max)^2), zero when max is zero.
+void launch_scaled_norm(cudaStream_t s, int n, const double* v, Scalars* scalars,
+                        double* partials);
 void launch_copy(cudaStream_t s, int n, const double* src, double* dst);
 // ---- the steps either side of the solve ----------------------------------------
 // Pressure-correction system assembly (diag, rhs) from densities, the

@@ -1073,6 +1073,19 @@ Status Solver::sync_scalars() {
   return {};
 }
 
+// The solve's 2-norm of a vector whose plain sum of squares a kernel has just
+// formed: queue_norm adds the two max-scaled passes when the solve asked for
+// the reference's global_norm (HFPS_NORM_SCALED); norm_value reads whichever
+// form after the scalars are back on the host.
+void Solver::queue_norm(const double* v) {
+  if (!scaled_norm_) return;
+  launch_scaled_norm(stream_, nx_ * ny_ * nz_, v, d_scalars_, d_partials_);
+  launches_ += 2;
+}
+double Solver::norm_value(double plain_squares) const {
+  return scaled_norm_ ? h_scalars_->misc[3] : std::sqrt(plain_squares);
+}
+
 // solve_pcg (src/solver_krylov.cpp:1299-1555) with identical control flow:
 // true residual every `true_residual_interval` iterations, at a recursive
 // convergence claim and at the cap, and a restart of the search direction
@@ -1087,13 +1100,14 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
   if (!st) return st;
   launch_norm2(stream_, n, kb_, red(kOpMisc));
   launches_ += 1;
+  queue_norm(kb_);
   st = sync_scalars();
   if (!st) return st;
   if (h_scalars_->flags & 1) {
     result.termination = HFPS_NON_FINITE;
     return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite rhs");
   }
-  const double bnorm = std::sqrt(h_scalars_->misc[0]);
+  const double bnorm = norm_value(h_scalars_->misc[0]);
   const double tol = std::max(control.absolute_tolerance,
                               control.relative_tolerance * bnorm);
   result.rhs_norm = bnorm;
@@ -1106,9 +1120,10 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
   launch_residual_norm(stream_, A, kx_, kb_, kr_, red(kOpRecursive));
   launches_ += 1;
   ++result.operator_applies;
+  queue_norm(kr_);
   st = sync_scalars();
   if (!st) return st;
-  result.initial_true_residual = std::sqrt(h_scalars_->rr);
+  result.initial_true_residual = norm_value(h_scalars_->rr);
   result.final_true_residual = result.initial_true_residual;
   result.recursive_residual = result.initial_true_residual;
   if (!std::isfinite(result.initial_true_residual)) {
@@ -1152,6 +1167,7 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
     ++result.operator_applies;
     launch_pcg_update(stream_, n, kx_, kp_, kr_, kap_, red(kOpRecursive));
     launches_ += 2;
+    queue_norm(kr_);
     ++it;
     const bool planned = it % control.true_residual_interval == 0 ||
                          it == control.maximum_iterations;
@@ -1191,7 +1207,7 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
       result.termination = HFPS_NON_FINITE;
       return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite Krylov scalar");
     }
-    const double recursive = std::sqrt(h_scalars_->rr);
+    const double recursive = norm_value(h_scalars_->rr);
     result.recursive_residual = recursive;
     last_recursive = recursive;
     if (history != nullptr && it - 1 < capacity) {
@@ -1203,9 +1219,10 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
       launch_residual_norm(stream_, A, kx_, kb_, kr_, red(kOpRecursive));
       launches_ += 1;
       ++result.operator_applies;
+      queue_norm(kr_);
       st = sync_scalars();
       if (!st) return st;
-      result.final_true_residual = std::sqrt(h_scalars_->rr);
+      result.final_true_residual = norm_value(h_scalars_->rr);
       result.recursive_residual = result.final_true_residual;
       if (result.final_true_residual <= tol) {
         result.termination = HFPS_CONVERGED;
@@ -1393,9 +1410,10 @@ Status Solver::recycle_project(const hfps_control& control, double tol, hfps_res
   launch_basis_update(stream_, n, kx_, dir, 1.0, false, candidate);
   launch_residual_norm(stream_, A, candidate, kb_, fg_w_, red(kOpRecursive));
   launches_ += 2;
+  queue_norm(fg_w_);
   st = sync_scalars();
   if (!st) return st;
-  const double candidate_norm = std::sqrt(h_scalars_->rr);
+  const double candidate_norm = norm_value(h_scalars_->rr);
   result.recycle_projected_residual = candidate_norm;
   if (std::isfinite(candidate_norm) && candidate_norm < result.final_true_residual) {
     launch_copy(stream_, n, candidate, kx_);
@@ -1456,13 +1474,14 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
   if (!st) return st;
   launch_norm2(stream_, n, kb_, red(kOpMisc));
   launches_ += 1;
+  queue_norm(kb_);
   st = sync_scalars();
   if (!st) return st;
   if (h_scalars_->flags & 1) {
     result.termination = HFPS_NON_FINITE;
     return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite rhs");
   }
-  const double bnorm = std::sqrt(h_scalars_->misc[0]);
+  const double bnorm = norm_value(h_scalars_->misc[0]);
   const double tol = std::max(control.absolute_tolerance,
                               control.relative_tolerance * bnorm);
   result.rhs_norm = bnorm;
@@ -1480,9 +1499,10 @@ Status Solver::krylov_fgmres(const hfps_control& control, hfps_result& result,
     launch_residual_norm(stream_, A, x, kb_, r, red(kOpRecursive));
     launches_ += 1;
     ++result.operator_applies;
+    queue_norm(r);
     Status s = sync_scalars();
     if (!s) return s;
-    norm = std::sqrt(h_scalars_->rr);
+    norm = norm_value(h_scalars_->rr);
     if (!std::isfinite(norm)) {
       result.termination = HFPS_NON_FINITE;
       return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite residual");
@@ -1790,13 +1810,14 @@ Status Solver::krylov_bicgstab(const hfps_control& control, hfps_result& result,
   if (!st) return st;
   launch_norm2(stream_, n, kb_, red(kOpMisc));
   launches_ += 1;
+  queue_norm(kb_);
   st = sync_scalars();
   if (!st) return st;
   if (h_scalars_->flags & 1) {
     result.termination = HFPS_NON_FINITE;
     return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite rhs");
   }
-  const double bnorm = std::sqrt(h_scalars_->misc[0]);
+  const double bnorm = norm_value(h_scalars_->misc[0]);
   const double tol = std::max(control.absolute_tolerance, control.relative_tolerance * bnorm);
   result.rhs_norm = bnorm;
   result.true_residual_limit = tol;
@@ -1809,9 +1830,10 @@ Status Solver::krylov_bicgstab(const hfps_control& control, hfps_result& result,
     launch_residual_norm(stream_, A, kx_, kb_, r, red(kOpRecursive));
     launches_ += 1;
     ++result.operator_applies;
+    queue_norm(r);
     Status s2 = sync_scalars();
     if (!s2) return s2;
-    norm = std::sqrt(h_scalars_->rr);
+    norm = norm_value(h_scalars_->rr);
     if (!std::isfinite(norm)) {
       result.termination = HFPS_NON_FINITE;
       return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite residual");
@@ -1888,9 +1910,10 @@ Status Solver::krylov_bicgstab(const hfps_control& control, hfps_result& result,
     alpha = rho / denominator;
     launch_bicg_intermediate(stream_, n, sv, r, v, alpha, red(kOpMisc));
     launches_ += 1;
+    queue_norm(sv);
     st = sync_scalars();
     if (!st) return st;
-    const double s_norm = std::sqrt(h_scalars_->misc[0]);
+    const double s_norm = norm_value(h_scalars_->misc[0]);
     if (!std::isfinite(s_norm)) {
       result.termination = HFPS_NON_FINITE;
       return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite BiCGSTAB residual");
@@ -1932,11 +1955,12 @@ Status Solver::krylov_bicgstab(const hfps_control& control, hfps_result& result,
     if (omega == 0.0 || !std::isfinite(omega)) return breakdown();
     launch_bicg_update(stream_, n, kx_, ph, sh, r, sv, t, alpha, omega, red(kOpRecursive));
     launches_ += 1;
+    queue_norm(r);
     ++it;
     result.iterations = it;
     st = sync_scalars();
     if (!st) return st;
-    const double recursive = std::sqrt(h_scalars_->rr);
+    const double recursive = norm_value(h_scalars_->rr);
     if (!std::isfinite(recursive)) {
       result.termination = HFPS_NON_FINITE;
       return fail(HFPS_NUMERICAL_FAILURE, kDetailNumeric, "non-finite BiCGSTAB residual");
@@ -1983,6 +2007,7 @@ Status Solver::solve(const double* rhs, double* solution, int memory,
       control.relative_tolerance < 0.0 || control.absolute_tolerance < 0.0 ||
       (control.relative_tolerance == 0.0 && control.absolute_tolerance == 0.0) ||
       (control.precision != HFPS_FP64 && control.precision != HFPS_MIXED) ||
+      (control.norm != HFPS_NORM_PLAIN && control.norm != HFPS_NORM_SCALED) ||
       control.recycle < HFPS_RECYCLE_NONE || control.recycle > HFPS_RECYCLE_GUARD ||
       (control.algorithm == HFPS_PCG && control.recycle != HFPS_RECYCLE_NONE) ||
       (control.algorithm != HFPS_FGMRES && control.recycle != HFPS_RECYCLE_NONE) ||
@@ -1998,6 +2023,7 @@ Status Solver::solve(const double* rhs, double* solution, int memory,
   if (st) st = copy_in(kx_, solution, n, memory);
   if (!st) return st;
   launches_ = 0;
+  scaled_norm_ = control.norm == HFPS_NORM_SCALED;
   st = control.algorithm == HFPS_FGMRES     ? krylov_fgmres(control, result, history, capacity)
        : control.algorithm == HFPS_BICGSTAB ? krylov_bicgstab(control, result, history, capacity)
                                             : krylov_pcg(control, result, history, capacity);

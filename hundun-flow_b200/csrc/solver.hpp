@@ -189,6 +189,9 @@ class Solver {
   int tail_steps_{-1};
   int tail_blocks_[2]{};
   bool tail_barrier_test_{false};
+  bool scaled_norm_{false};   // the current solve's hfps_control.norm is SCALED
+  void queue_norm(const double* v);
+  double norm_value(double plain_squares) const;
   // FGMRES basis: V_0..V_restart, Z_0..Z_{restart-1} and the operator image,
   // allocated on first use for the largest restart asked for.
   double* fg_storage_{};

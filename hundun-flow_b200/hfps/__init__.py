@@ -6,5 +6,6 @@ of include/hf_pressure_solver.h; this package is its thin Python mirror
 and a torch.autograd wrapper used for gradient checks (``autograd``).
 """
 from . import workloads  # noqa: F401
-from .solver import (BICGSTAB, DEVICE, FGMRES, FP64, HOST, IC0, MG, MIXED, PCG,  # noqa: F401
-                     Policy, PressureSolver, SolveOptions, SolverError, library_path)
+from .solver import (BICGSTAB, DEVICE, FGMRES, FP64, HOST, IC0, MG, MIXED, NORM_PLAIN,  # noqa: F401
+                     NORM_SCALED, PCG, Policy, PressureSolver, SolveOptions, SolverError,
+                     library_path)

@@ -25,6 +25,7 @@ LIBRARY = os.path.join(PACKAGE, "libhfps.so")
 HOST, DEVICE = 0, 1
 FP64, MIXED = 0, 1
 PCG, FGMRES, BICGSTAB = 0, 1, 2
+NORM_PLAIN, NORM_SCALED = 0, 1
 MG, IC0 = 0, 1
 RECYCLE = {"none": 0, "capture": 1, "project": 2, "guard": 3}
 
@@ -91,7 +92,8 @@ class Control(ctypes.Structure):
                 ("maximum_iterations", ctypes.c_uint32),
                 ("true_residual_interval", ctypes.c_uint32),
                 ("restart", ctypes.c_uint32), ("algorithm", ctypes.c_int),
-                ("precision", ctypes.c_int), ("recycle", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("recycle", ctypes.c_int),
+                ("norm", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
@@ -229,6 +231,7 @@ class SolveOptions:
     algorithm: int = PCG   # PCG (solve_pcg) or FGMRES (solve_fgmres)
     restart: int = 0       # FGMRES restart length (the reference's default is 12)
     recycle: str = "none"  # FGMRES: "none", "capture", "project", "guard"
+    norm: int = 0          # NORM_PLAIN, or NORM_SCALED (the reference's max-scaled global_norm)
 
 
 class PressureSolver:
@@ -413,6 +416,7 @@ class PressureSolver:
         if options.algorithm == FGMRES and c.restart == 0:
             c.restart = 12
         c.recycle = RECYCLE[options.recycle]
+        c.norm = options.norm
         return c
 
     def solve(self, rhs, x0=None, options: Optional[SolveOptions] = None, out=None,

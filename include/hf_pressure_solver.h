@@ -125,7 +125,20 @@ typedef struct hfps_control {
   int algorithm;      /* hfps_algorithm */
   int precision;      /* hfps_precision */
   int recycle;        /* hfps_recycle (FGMRES only) */
+  int norm;           /* hfps_norm */
 } hfps_control;
+
+/* How the solve forms the 2-norms of rhs and residuals.  PLAIN (default):
+ * sqrt of a fixed-order FP64 sum of squares, fused into the kernel that
+ * produces the vector.  SCALED: the reference's global_norm
+ * (src/solver_krylov.cpp:650-711): max |v| first, then max * sqrt(sum of
+ * (v / max)^2), in two extra passes; used for ||b||, every true residual and
+ * the recursive residuals of PCG and BiCGSTAB.  The Arnoldi norms of FGMRES
+ * keep their own form (its Pythagorean update with fallbacks). */
+typedef enum hfps_norm {
+  HFPS_NORM_PLAIN = 0,
+  HFPS_NORM_SCALED = 1
+} hfps_norm;
 
 /* Subspace recycling across consecutive pressure solves (FGMRES only), as
  * PressureVelocityCoupler selects it per corrector (src/solver_piso.cpp:

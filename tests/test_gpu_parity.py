@@ -260,3 +260,35 @@ def test_beta_helper_matches_host_assembly(hfps_mod):
     h = hfps_mod.PressureSolver.from_system(s, hfps_mod.Policy.production())
     for a, b in zip(g.level_coefficients(0), h.level_coefficients(0)):
         assert rel(a, b) <= 1e-14
+
+
+def test_scaled_norm_matches_global_norm(hfps_mod):
+    """HFPS_NORM_SCALED forms ||b|| and every residual norm as the reference's
+    global_norm (src/solver_krylov.cpp:650-711): max |v|, then
+    max * sqrt(sum (v / max)^2).  The rhs norm matches that definition
+    evaluated exactly (math.fsum) to a few ulps, and PCG, FGMRES and the
+    BiCGSTAB cold path reach the same solutions in the same iterations as
+    with the plain norm; a zero rhs still terminates as zero_rhs."""
+    import math
+    s = workloads.make("wrinkled256", n=(48, 64, 32))
+    b = s.rhs.reshape(-1)
+    m = float(np.max(np.abs(b)))
+    exact = m * math.sqrt(math.fsum(float(v) * float(v) for v in (b / m)))
+    runs = [(hfps_mod.Policy.production(), dict()),
+            (hfps_mod.Policy.production().replace(unit_linear=0),
+             dict(algorithm=hfps_mod.FGMRES, restart=12)),
+            (hfps_mod.Policy.production().replace(preconditioner=hfps_mod.IC0),
+             dict(algorithm=hfps_mod.BICGSTAB))]
+    for policy, extra in runs:
+        g = hfps_mod.PressureSolver.from_system(s, policy)
+        x0, i0 = g.solve(s.rhs, rtol=1e-11, maxit=800, **extra)
+        x1, i1 = g.solve(s.rhs, rtol=1e-11, maxit=800, norm=hfps_mod.NORM_SCALED, **extra)
+        assert i1["termination"] == "converged"
+        assert abs(i1["rhs_norm"] - exact) <= 4e-16 * 8 * exact
+        assert abs(i0["rhs_norm"] - i1["rhs_norm"]) <= 1e-14 * exact
+        assert abs(i1["iterations"] - i0["iterations"]) <= 1
+        assert i1["final_true_residual"] <= i1["true_residual_limit"]
+        assert np.linalg.norm(x1 - x0) <= 1e-9 * np.linalg.norm(x0)
+        _, z = g.solve(np.zeros_like(s.rhs), norm=hfps_mod.NORM_SCALED, **extra)
+        assert z["termination"] == "zero_rhs"
+        g.close()
