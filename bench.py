@@ -78,7 +78,9 @@ def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    # The reference arm runs on rank 0's host cores alone and takes no
+    # collective step, so its ranks join no process group.
+    if world > 1 and args.impl != "reference":
         import datetime
         import torch
         import torch.distributed as dist
@@ -710,8 +712,8 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args, world, rank)
-    else:
-        run_b200(args, world, rank, local)
+        return
+    run_b200(args, world, rank, local)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

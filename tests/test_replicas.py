@@ -60,3 +60,18 @@ def test_replica_value_is_aggregate_over_ranks():
     src = inspect.getsource(bench.run_b200)
     assert "value = world * args.steps / seconds" in src
     assert "max_over_ranks(world" in src
+
+
+def test_reference_arm_ranks_join_no_process_group(monkeypatch):
+    """Under torchrun the reference arm's ranks take no collective step, so
+    they create no process group: rank 0 runs the reference's CPU solve
+    alone and the other ranks exit at once, with nothing left to shut down."""
+    import argparse
+    import bench
+    import torch.distributed as dist
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    monkeypatch.setenv("RANK", "1")
+    monkeypatch.setenv("LOCAL_RANK", "1")
+    world, rank, local = bench.dist_setup(argparse.Namespace(impl="reference"))
+    assert (world, rank, local) == (2, 1, 1)
+    assert not dist.is_initialized()
