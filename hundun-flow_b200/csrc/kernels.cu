@@ -13,7 +13,6 @@
 
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 
 namespace hfps {
 namespace {
@@ -1586,13 +1585,11 @@ void launch_mg_projection(cudaStream_t s, int n, const double* r,
 }
 
 // The tiled operator serves grids whose tile count fits the reduction
-// partials; HFPS_TILED_STENCIL=0 keeps the row-walking kernel.
-bool use_tiled_stencil(const Level<double>& L) {
-  const char* env = std::getenv("HFPS_TILED_STENCIL");
-  const bool enabled = !(env != nullptr && env[0] == '0');
+// partials.
+bool tiles_fit(const Level<double>& L) {
   const long long tiles = static_cast<long long>((L.nx + kTileX - 1) / kTileX) *
                           ((L.ny + kTileY - 1) / kTileY) * ((L.nz + kTileZ - 1) / kTileZ);
-  return enabled && tiles <= kMaxTiledBlocks;
+  return tiles <= kMaxTiledBlocks;
 }
 int tiled_blocks(const Level<double>& L) {
   return ((L.nx + kTileX - 1) / kTileX) * ((L.ny + kTileY - 1) / kTileY) *
@@ -1600,8 +1597,8 @@ int tiled_blocks(const Level<double>& L) {
 }
 
 void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
-                     double* y, Reduce red) {
-  if (use_tiled_stencil(L)) {
+                     double* y, Reduce red, bool tiled) {
+  if (tiled && tiles_fit(L)) {
     launch(k_stencil_tiled, tiled_blocks(L), kTileX * kTileY, 0, s, L, x, y, red);
     return;
   }

@@ -205,8 +205,10 @@ void launch_mg_projection(cudaStream_t s, int n, const double* r,
                           Reduce red);
 
 // ---- Krylov (FP64) --------------------------------------------------------
+// y = A x and x.y: over 3-D shared-memory tiles when `tiled` and the tiles'
+// partial sums fit the partials block, else a warp per x-row (the same rows).
 void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
-                     double* y, Reduce red);
+                     double* y, Reduce red, bool tiled = true);
 void launch_residual_norm(cudaStream_t s, const Level<double>& L,
                           const double* x, const double* b, double* r,
                           Reduce red);

@@ -352,6 +352,10 @@ Status Solver::allocate() {
     // host reads each iteration's scalars before queueing more work).
     const char* ahead = std::getenv("HFPS_QUEUE_AHEAD");
     queue_ahead_ = !(ahead != nullptr && ahead[0] == '0');
+    // The Krylov operator over 3-D tiles (HFPS_TILED_STENCIL=0: the row
+    // kernel; the same rows, another grouping of the p.Ap partials).
+    const char* tiled = std::getenv("HFPS_TILED_STENCIL");
+    tiled_stencil_ = !(tiled != nullptr && tiled[0] == '0');
   }
   st = check(cudaEventCreateWithFlags(&scalars_ready_, cudaEventDisableTiming), "event");
   if (!st) return st;
@@ -1163,7 +1167,7 @@ Status Solver::krylov_pcg(const hfps_control& control, hfps_result& result,
   constexpr double kQueueAheadMargin = 8.0;
   double last_recursive = result.initial_true_residual;
   while (it < control.maximum_iterations) {
-    launch_spmv_dot(stream_, A, kp_, kap_, red(kOpPap));
+    launch_spmv_dot(stream_, A, kp_, kap_, red(kOpPap), tiled_stencil_);
     ++result.operator_applies;
     launch_pcg_update(stream_, n, kx_, kp_, kr_, kap_, red(kOpRecursive));
     launches_ += 2;
@@ -2172,7 +2176,7 @@ Status Solver::profile_kernel(int kernel, int repetitions, double* ms,
   const auto one = [&]() {
     switch (kernel) {
       case HFPS_KERNEL_OPERATOR:
-        launch_spmv_dot(stream_, A, kp_, kap_, red(kOpMisc));
+        launch_spmv_dot(stream_, A, kp_, kap_, red(kOpMisc), tiled_stencil_);
         per_cell = 48.0;
         break;
       case HFPS_KERNEL_SMOOTH_FP64:

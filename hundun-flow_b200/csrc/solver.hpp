@@ -165,6 +165,7 @@ class Solver {
   double* kb_{};
   bool krylov_fusion_{true};  // PCG's r.z formed in the MG exit
   bool queue_ahead_{true};    // PCG queues the next MG before reading scalars
+  bool tiled_stencil_{true};  // the Krylov operator over 3-D tiles
   cudaEvent_t scalars_ready_{};  // the scalar readback of the current step
   Scalars* d_scalars_{};
   Scalars* h_scalars_{};      // pinned

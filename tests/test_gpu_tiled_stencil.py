@@ -1,5 +1,6 @@
 """The Krylov operator over 3-D tiles (k_stencil_tiled: A p with p.Ap)
-against the row-walking kernel (HFPS_TILED_STENCIL=0, read at every launch).
+against the row-walking kernel (HFPS_TILED_STENCIL=0, read when the solver
+is created).
 Rows are evaluated in the same order, so only the grouping of the
 reduction partials differs: PCG and FGMRES solves take the same iteration
 count (+-1) and agree to 1e-10, on even and ragged extents (partial tiles in
