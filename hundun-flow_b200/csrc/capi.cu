@@ -56,6 +56,7 @@ void hfps_default_policy(hfps_policy* p) {
   p->anisotropy_threshold = 4.0;
   p->diagonal_shortcut_maximum_ratio = 0.0;
   p->preconditioner = HFPS_PRECONDITIONER_MG;
+  p->null_space = HFPS_NULL_SPACE_NONE;
 }
 
 void hfps_production_policy(hfps_policy* p) {

@@ -997,6 +997,40 @@ __global__ void k_norm_scaled_sum(int n, const double* __restrict__ a, Reduce re
     apply_scalar_op(red.scalars, red.op, v[0]);
 }
 
+// The two passes of project_constant: the volume-weighted sums (FP64, in
+// the fixed-order tree; the reference adds them cell by cell), then the
+// subtraction, formed in FP64 and stored in the level's precision.
+template <class T>
+__global__ void k_constant_sums(int n, VecLayout lay, const T* __restrict__ v,
+                                const double* __restrict__ volume, Reduce red) {
+  grid_dependency_sync();
+  double acc[2] = {0.0, 0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const double w = volume[c];
+    acc[0] += w * static_cast<double>(v[vec_pos(lay, c)]);
+    acc[1] += w;
+  }
+  if (finish_reduction<2>(acc, red) && threadIdx.x == 0) {
+    Scalars* sc = red.scalars;
+    sc->constant_mean = acc[0] / acc[1];
+    if (!(acc[1] > 0.0) || !isfinite(acc[0]) || !isfinite(acc[1])) sc->flags |= 1;
+  }
+}
+
+template <class T>
+__global__ void k_constant_apply(int n, VecLayout lay, T* __restrict__ v,
+                                 const double* __restrict__ volume,
+                                 const Scalars* __restrict__ sc) {
+  grid_dependency_sync();
+  const double mean = sc->constant_mean;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += gridDim.x * blockDim.x) {
+    const int at = vec_pos(lay, c);
+    v[at] = volume[c] > 0.0 ? static_cast<T>(static_cast<double>(v[at]) - mean) : T(0);
+  }
+}
+
 __global__ void k_p_update(int n, double* __restrict__ p,
                            const double* __restrict__ z,
                            const Scalars* __restrict__ sc) {
@@ -1627,6 +1661,20 @@ void launch_scaled_norm(cudaStream_t s, int n, const double* v, Scalars* scalars
   launch(k_norm_scaled_sum, reduction_blocks(n), kThreads, 0, s, n, v,
          Reduce{scalars, partials, kOpScaledNorm});
 }
+template <class T>
+void launch_project_constant(cudaStream_t s, int nx, int ny, int nz, int hx, T* v,
+                             const double* volume, Scalars* scalars, double* partials) {
+  const int n = nx * ny * nz;
+  const VecLayout lay{nx, ny, hx};
+  launch(k_constant_sums<T>, reduction_blocks(n), kThreads, 0, s, n, lay,
+         static_cast<const T*>(v), volume, Reduce{scalars, partials, kCounterProjectConstant});
+  launch(k_constant_apply<T>, grid_for(n), kThreads, 0, s, n, lay, v, volume,
+         static_cast<const Scalars*>(scalars));
+}
+template void launch_project_constant<double>(cudaStream_t, int, int, int, int, double*,
+                                              const double*, Scalars*, double*);
+template void launch_project_constant<float>(cudaStream_t, int, int, int, int, float*,
+                                             const double*, Scalars*, double*);
 void launch_p_update(cudaStream_t s, int n, double* p, const double* z,
                      const Scalars* sc) {
   launch(k_p_update, grid_for(n), kThreads, 0, s, n, p, z, sc);

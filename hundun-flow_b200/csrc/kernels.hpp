@@ -30,7 +30,8 @@ struct Scalars {
   int flags;         // bit 0 non-finite, bit 1 breakdown, bit 2 invalid assembly input,
                      // bit 3 a grid barrier of the small-level kernel timed out
   unsigned marks;    // bit 0: a difference had a nonzero entry (recycle capture)
-  unsigned counters[8];  // last-block arrival counters, one per reduction
+  unsigned counters[12];  // last-block arrival counters, one per reduction
+  double constant_mean;   // volume-weighted mean of the last project_constant
   // The small-level kernel's grid barrier: arrivals (on a 128-byte line of
   // its own).
   unsigned tail_pad0[32];
@@ -47,9 +48,11 @@ enum ScalarOp : int {
   kOpScaledNorm = 7, // misc[3] = misc[2] * sqrt(sum): the max-scaled norm (counter 7)
 };
 // Arrival counters of reductions that apply no scalar op: 5 MG projection,
-// 6 FGMRES multidot.  Counter 7 serves both passes of the max-scaled norm.
+// 6 FGMRES multidot, 8 project_constant.  Counter 7 serves both passes of
+// the max-scaled norm.
 constexpr int kCounterProjection = 5;
 constexpr int kCounterMultidot = 6;
+constexpr int kCounterProjectConstant = 8;
 constexpr int kMaxFgmresRestart = 64;
 
 struct Reduce {
@@ -203,6 +206,14 @@ template <class T>
 void launch_mg_projection(cudaStream_t s, int n, const double* r,
                           const uint8_t* active, const T* recursive,
                           Reduce red);
+
+// project_constant (src/solver_mg.cpp:1411-1453) on a level vector v in
+// layout hx: v - mean on cells of positive volume and 0 on the others, mean
+// = sum(volume v) / sum(volume) (kept in scalars->constant_mean).  A total
+// volume that is not positive or a non-finite sum sets flag bit 0.
+template <class T>
+void launch_project_constant(cudaStream_t s, int nx, int ny, int nz, int hx, T* v,
+                             const double* volume, Scalars* scalars, double* partials);
 
 // ---- Krylov (FP64) --------------------------------------------------------
 // y = A x and x.y: over 3-D shared-memory tiles when `tiled` and the tiles'

@@ -103,7 +103,8 @@ bool valid_policy(const hfps_policy& p) {
          std::isfinite(p.diagonal_shortcut_maximum_ratio) &&
          p.diagonal_shortcut_maximum_ratio >= 0.0 &&
          p.diagonal_shortcut_maximum_ratio < 1.0 &&
-         (p.unit_linear == 0 || p.unit_linear == 1);
+         (p.unit_linear == 0 || p.unit_linear == 1) &&
+         (p.null_space == HFPS_NULL_SPACE_NONE || p.null_space == HFPS_NULL_SPACE_CONSTANT);
 }
 
 }  // namespace
@@ -497,7 +498,8 @@ Status Solver::build_hierarchy() {
   select_tail();
   // Diagonal shortcut (select_diagonal_shortcut, src/solver_mg.cpp:1577-1611).
   diagonal_shortcut_ = false;
-  if (policy_.diagonal_shortcut_maximum_ratio != 0.0) {
+  if (policy_.diagonal_shortcut_maximum_ratio != 0.0 &&
+      policy_.null_space == HFPS_NULL_SPACE_NONE) {
     const Level<double> L0 = l64_[0].view(neumann_);
     launch_shortcut_ratio(stream_, L0, Reduce{d_scalars_, d_partials_, kOpMisc});
     const int blocks = reduction_blocks(static_cast<long long>(L0.nx) * L0.ny * L0.nz);
@@ -811,7 +813,7 @@ void Solver::select_tail() {
   // that path; the GPU stays usable).
   const char* test = std::getenv("HFPS_TAIL_BARRIER_TEST");
   tail_barrier_test_ = test != nullptr && test[0] == '1';
-  if (!on || !coarse_dense_) return;
+  if (!on || !coarse_dense_ || policy_.null_space != HFPS_NULL_SPACE_NONE) return;
   const int levels = static_cast<int>(l64_.size());
   int first = levels - 1;
   int axis = -1, extent = -1;
@@ -922,6 +924,10 @@ void Solver::cycle(std::vector<DeviceLevel<T>>& levels, int level, int counter,
   // Retained defect + restrict_residual in one pass.
   launch_defect_restrict<T>(stream_, F.view(neumann_), F.x, F.b, C.view(neumann_),
                             C.b, C.x, F.coarsen_mask, F.split, C.split);
+  // restrict_residual's projection of the coarse rhs (src/solver_mg.cpp:3708-3716).
+  if (policy_.null_space == HFPS_NULL_SPACE_CONSTANT)
+    launch_project_constant<T>(stream_, C.nx, C.ny, C.nz, C.split, C.b, volume_[level + 1],
+                               d_scalars_, d_partials_);
   if (level + 1 == tail_level_) {
     // Both visits of the level below (an F-cycle's counter 2 and 1) in one
     // persistent launch.
@@ -967,11 +973,20 @@ void Solver::mg_enqueue(std::vector<DeviceLevel<T>>& levels, const double* r,
   // pre-smoothing sweep (zero flags) defines every entry anyway.
   const bool zero_x = !(diagonal_shortcut_ || first_sweep_zero_);
   launch_mg_enter<T>(stream_, n, r, d_active_, L0.b, L0.x, v0, zero_x);
+  // MgNullSpace::constant: the rhs, every restricted rhs and the result lose
+  // their volume-weighted mean (apply_impl, src/solver_mg.cpp:4900-4960).
+  const bool constant = policy_.null_space == HFPS_NULL_SPACE_CONSTANT;
+  if (constant)
+    launch_project_constant<T>(stream_, L0.nx, L0.ny, L0.nz, L0.split, L0.b, volume_[0],
+                               d_scalars_, d_partials_);
   if (diagonal_shortcut_) {
     launch_diagonal_solve<T>(stream_, n, L0.b, L0.diag, L0.x, v0);
   } else {
     cycle(levels, 0, policy_.cycle == 1 ? 2 : 1, true);
   }
+  if (constant)
+    launch_project_constant<T>(stream_, L0.nx, L0.ny, L0.nz, L0.split, L0.x, volume_[0],
+                               d_scalars_, d_partials_);
   if (policy_.unit_linear && krylov_fusion_) {
     // The PCG consumes r.z of every preconditioner application: formed here
     // while z is written (kOpRhoNext; the PCG's restarts use only rho).

@@ -54,7 +54,7 @@ class Policy(ctypes.Structure):
                 ("chebyshev_lower_spectrum_fraction", ctypes.c_double),
                 ("anisotropy_threshold", ctypes.c_double),
                 ("diagonal_shortcut_maximum_ratio", ctypes.c_double),
-                ("preconditioner", ctypes.c_int)]
+                ("preconditioner", ctypes.c_int), ("null_space", ctypes.c_int)]
 
     @staticmethod
     def default() -> "Policy":

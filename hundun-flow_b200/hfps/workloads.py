@@ -228,8 +228,10 @@ PISO_BOUNDARY = (NEUMANN, DIRICHLET, NEUMANN, NEUMANN, NEUMANN, NEUMANN)
 
 def spherical_flame(n: Sequence[int] = (64, 64, 64), thickness: float = 0.02,
                     spheres=((0.3, 0.5, 0.5, 0.1),), seed: int = 0,
-                    name: str = "spherical_flame") -> PressureSystem:
-    """Density-ratio-7 spherical flame with solid IBM spheres (64^3 case)."""
+                    name: str = "spherical_flame", boundary=PISO_BOUNDARY) -> PressureSystem:
+    """Density-ratio-7 spherical flame with solid IBM spheres (64^3 case).
+    ``boundary`` all NEUMANN gives a singular, consistent system (constant
+    null space)."""
     nx, ny, nz = n
     faces = (uniform_faces(nx), uniform_faces(ny), uniform_faces(nz))
     z, y, x = _grid(faces)
@@ -238,7 +240,7 @@ def spherical_flame(n: Sequence[int] = (64, 64, 64), thickness: float = 0.02,
     solid = np.zeros((nz, ny, nx), bool)
     for (sx, sy, sz, sr) in spheres:
         solid |= (x - sx) ** 2 + (y - sy) ** 2 + (z - sz) ** 2 <= sr * sr
-    return _build(name, faces, rho, solid, PISO_BOUNDARY, seed,
+    return _build(name, faces, rho, solid, tuple(boundary), seed,
                   {"thickness": thickness, "spheres": spheres})
 
 

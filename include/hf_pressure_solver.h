@@ -100,7 +100,19 @@ typedef struct hfps_policy {
   double anisotropy_threshold;              /* default 4.0 */
   double diagonal_shortcut_maximum_ratio;   /* default 0.0 (off) */
   int preconditioner;                       /* hfps_preconditioner, default MG */
+  int null_space;                           /* hfps_null_space, default NONE */
 } hfps_policy;
+
+/* MgNullSpace (include/hundun/v04_linear.hpp:104).  CONSTANT, for a system
+ * whose operator annihilates constants (every boundary Neumann): the MG
+ * application removes the volume-weighted mean from its level-0 rhs, from
+ * every restricted coarse rhs and from its result (project_constant,
+ * src/solver_mg.cpp:1411-1453, 3708-3716, 4900-4960), and the diagonal
+ * shortcut is not taken.  The rhs must be consistent (zero-sum). */
+typedef enum hfps_null_space {
+  HFPS_NULL_SPACE_NONE = 0,
+  HFPS_NULL_SPACE_CONSTANT = 1
+} hfps_null_space;
 
 /* Cartesian geometry: face coordinates per axis (n+1 values each),
  * boundary kinds [x_min, x_max, y_min, y_max, z_min, z_max] and an optional

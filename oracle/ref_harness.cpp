@@ -250,7 +250,8 @@ extern "C" {
 // options: [algorithm(0 pcg,1 fgmres,2 bicgstab), restart, smoother(0 red-black,
 //           1 chebyshev), cycle(0 V,1 F), pre, post, coarse_sweeps,
 //           scaling(0 residual-minimising, 1 unit_linear), max_levels,
-//           minimum_coarse_extent, preconditioner(0 MG plan, 1 ICCG, 2 DILU)]
+//           minimum_coarse_extent, preconditioner(0 MG plan, 1 ICCG, 2 DILU),
+//           null_space(0 none, 1 constant)]
 // reals:   [chebyshev_lower_spectrum_fraction, anisotropy_threshold,
 //           diagonal_shortcut_maximum_ratio]
 // Returns 0 on success, otherwise status code * 100000 + detail.
@@ -362,7 +363,7 @@ int hfref_create(int nx, int ny, int nz, const double* x_faces,
   spec.geometry = &s.geometry;
   spec.patch = s.patch;
   spec.boundaries = boundaries;
-  spec.null_space = MgNullSpace::none;
+  spec.null_space = options[11] == 1 ? MgNullSpace::constant : MgNullSpace::none;
   spec.operator_class = MgOperatorClass::symmetric_diagonally_dominant_m_matrix;
   spec.policy.point_smoother = options[2] == 1
                                    ? MgPointSmootherKind::chebyshev_jacobi

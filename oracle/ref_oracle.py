@@ -87,10 +87,11 @@ class RefSession:
 
     def __init__(self, system, policy: Optional[MgPolicy] = None, algorithm: str = "pcg",
                  restart: int = 12, unit_linear: Optional[bool] = None,
-                 preconditioner: str = "mg"):
+                 preconditioner: str = "mg", null_space: str = "none"):
         """``algorithm`` "pcg" / "fgmres" / "bicgstab"; ``preconditioner`` "mg"
         (the plan), "iccg" (ColdPressureIccg, with PCG) or "dilu"
-        (ColdPressureDilu, with BiCGSTAB)."""
+        (ColdPressureDilu, with BiCGSTAB); ``null_space`` "none" or "constant"
+        (MgNullSpace of the plan)."""
         lib = _load()
         self.system = system
         policy = policy or MgPolicy()
@@ -99,11 +100,12 @@ class RefSession:
         nx, ny, nz = system.shape
         self._faces = [np.ascontiguousarray(f, dtype=np.float64) for f in system.faces]
         self._bc = (ctypes.c_int * 6)(*system.boundary)
-        options = (ctypes.c_int * 11)(self.ALGORITHMS[algorithm], restart, policy.smoother,
+        options = (ctypes.c_int * 12)(self.ALGORITHMS[algorithm], restart, policy.smoother,
                                       policy.cycle, policy.pre, policy.post, policy.coarse_sweeps,
                                       1 if unit_linear else 0, policy.max_levels,
                                       policy.min_coarse_extent,
-                                      self.PRECONDITIONERS[preconditioner])
+                                      self.PRECONDITIONERS[preconditioner],
+                                      {"none": 0, "constant": 1}[null_space])
         reals = (ctypes.c_double * 3)(policy.chebyshev_fraction, policy.anisotropy_threshold,
                                       policy.diagonal_shortcut)
         active = None

@@ -6,6 +6,7 @@ Run in a tree where the reference sources are present:
     python tests/golden/make_golden.py --scale                          # 128^3, 256^3
     python tests/golden/make_golden.py --steps                          # assembly steps
     python tests/golden/make_golden.py --c2                             # 512x256x256
+    python tests/golden/make_golden.py --null-space                     # MgNullSpace::constant
 
 For each small case the script builds the seeded system with
 hfps.workloads, then records what the reference's own code returns for it
@@ -292,7 +293,47 @@ def steps_main():
         json.dump(index, f, indent=1)
 
 
+# A pure-Neumann system (every boundary Neumann: the operator annihilates
+# constants; the divergence rhs sums to zero) under MgNullSpace::constant.
+NULL_SPACE_CASE = dict(config="sphere64", n=(24, 20, 16), boundary=[1, 1, 1, 1, 1, 1])
+NULL_SPACE_POLICIES = {"rbV22": dict(), "prodF": dict(smoother=1, cycle=1, pre=1, post=2,
+                                                      diagonal_shortcut=0.1)}
+
+
+def null_space_main():
+    """The reference's MG application with the constant null space (both
+    policies, unit-scaled and residual-minimising), and its PCG (unit) and
+    FGMRES(12) (residual-minimising) solves at rtol 1e-13 from x0 = 0."""
+    system = system_for(NULL_SPACE_CASE)
+    v = probe_vector(system)
+    arrays, index = {}, {"spec": NULL_SPACE_CASE, "digest": input_digest(system)}
+    for tag, pol in NULL_SPACE_POLICIES.items():
+        policy = ref_oracle.MgPolicy(**pol)
+        ref = ref_oracle.RefSession(system, policy, algorithm="pcg", null_space="constant")
+        arrays[f"{tag}_mg"] = ref.apply_mg(v)
+        x, info = ref.solve(system.rhs, rtol=1e-13, maxit=400)
+        ref.close()
+        arrays[f"{tag}_x"] = x
+        fg = ref_oracle.RefSession(system, policy, algorithm="fgmres", restart=12,
+                                   null_space="constant")
+        arrays[f"{tag}_mg_residual_minimising"] = fg.apply_mg(v)
+        xf, infof = fg.solve(system.rhs, rtol=1e-13, maxit=400)
+        fg.close()
+        arrays[f"{tag}_x_fgmres"] = xf
+        index[tag] = {"policy": pol, "pcg_iterations": info["iterations"],
+                      "pcg_termination": info["termination"],
+                      "fgmres_iterations": infof["iterations"],
+                      "fgmres_termination": infof["termination"]}
+        print(tag, index[tag])
+    np.savez_compressed(os.path.join(HERE, "null_space.npz"), **arrays)
+    with open(os.path.join(HERE, "null_space.json"), "w") as f:
+        json.dump(index, f, indent=1)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "--null-space":
+        null_space_main()
+        raise SystemExit(0)
     if len(sys.argv) > 1 and sys.argv[1] == "--steps":
         steps_main()
         raise SystemExit(0)

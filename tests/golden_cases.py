@@ -118,3 +118,18 @@ STEPS_SCALES = (1.0, 0.7)
 
 def steps_arrays():
     return dict(np.load(os.path.join(GOLDEN, "pressure_steps.npz")))
+
+
+def null_space_index():
+    with open(os.path.join(GOLDEN, "null_space.json")) as f:
+        return json.load(f)
+
+
+def null_space_system():
+    """The pure-Neumann sphere of tests/golden/null_space.* (MgNullSpace::constant)."""
+    from hfps import workloads
+    spec = dict(null_space_index()["spec"])
+    cfg = spec.pop("config")
+    spec["n"] = tuple(spec["n"])
+    spec["boundary"] = tuple(spec["boundary"])
+    return workloads.make(cfg, **spec)
