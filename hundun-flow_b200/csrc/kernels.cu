@@ -489,13 +489,14 @@ __global__ void k_mg_enter(int n, const double* __restrict__ r,
                            const uint8_t* __restrict__ active,
                            T* __restrict__ b, T* __restrict__ x, VecLayout v, bool zero_x) {
   grid_dependency_sync();
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
+  // A warp per x-row: the split position of a cell is then the row's base
+  // plus its parity half, with no division per cell.
+  for_each_cell_by_rows(v.nx, v.ny, n / (v.nx * v.ny), [&](int i, int j, int k, int c) {
     const bool on = active == nullptr || active[c] != 0;
-    const int at = vec_pos(v, c);
+    const int at = v.hx == 0 ? c : 2 * v.hx * (j + v.ny * k) + (i & 1) * v.hx + (i >> 1);
     b[at] = on ? static_cast<T>(r[c]) : T(0);
     if (zero_x) x[at] = T(0);
-  }
+  });
 }
 
 template <class T>
@@ -505,11 +506,11 @@ __global__ void k_mg_exit(int n, const T* __restrict__ x,
                           double* __restrict__ z, VecLayout v) {
   grid_dependency_sync();
   const double scale = scale_ptr == nullptr ? 1.0 : *scale_ptr;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
+  for_each_cell_by_rows(v.nx, v.ny, n / (v.nx * v.ny), [&](int i, int j, int k, int c) {
     const bool on = active == nullptr || active[c] != 0;
-    z[c] = on ? static_cast<double>(x[vec_pos(v, c)]) * scale : 0.0;
-  }
+    const int at = v.hx == 0 ? c : 2 * v.hx * (j + v.ny * k) + (i & 1) * v.hx + (i >> 1);
+    z[c] = on ? static_cast<double>(x[at]) * scale : 0.0;
+  });
 }
 
 // MG exit with the PCG's r.z: z = active ? x : 0 (unit scaling) and the sum
