@@ -522,12 +522,25 @@ __global__ void k_mg_exit_dot(int n, const T* __restrict__ x,
                               VecLayout v, const double* __restrict__ r, Reduce red) {
   grid_dependency_sync();
   double acc[1] = {0.0};
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n;
-       c += gridDim.x * blockDim.x) {
+  // k_dot's cells per thread (grid stride), with the cell's row and x index
+  // carried from step to step instead of divided out of c each time.
+  const int stride = gridDim.x * blockDim.x;
+  const int row_step = stride / v.nx, i_step = stride - row_step * v.nx;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  int row = c / v.nx;
+  int i = c - row * v.nx;
+  for (; c < n; c += stride) {
     const bool on = active == nullptr || active[c] != 0;
-    const double zc = on ? static_cast<double>(x[vec_pos(v, c)]) * 1.0 : 0.0;
+    const int at = v.hx == 0 ? c : 2 * v.hx * row + (i & 1) * v.hx + (i >> 1);
+    const double zc = on ? static_cast<double>(x[at]) * 1.0 : 0.0;
     z[c] = zc;
     acc[0] += r[c] * zc;
+    row += row_step;
+    i += i_step;
+    if (i >= v.nx) {
+      i -= v.nx;
+      ++row;
+    }
   }
   if (finish_reduction<1>(acc, red) && threadIdx.x == 0)
     apply_scalar_op(red.scalars, red.op, acc[0]);
