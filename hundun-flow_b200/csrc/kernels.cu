@@ -661,22 +661,11 @@ __global__ void __launch_bounds__(kTileX * kTileY)
   int c = ic + nx * (jc + ny * k0);
   double x_prev = (on && k0 > 0) ? x[c - plane] : 0.0;
   double x_cur = on ? x[c] : 0.0;
-  double x_next = (on && k0 + 1 < nz) ? x[c + plane] : 0.0;
   double fz_lo = on ? L.fz[c] : 0.0;
   double acc[1] = {0.0};
   int buf = 0;
   for (int k = k0; k < k1; ++k, c += plane) {
-    // Loads of plane k+2 and of this plane's coefficients go out before the
-    // barrier, so a thread has two planes of x and a plane of faces in flight.
-    const double x_after = (on && k + 2 < nz && k + 1 < k1) ? x[c + 2 * plane] : 0.0;
-    const int fxi = face_x_index(L, c, j, k);
-    const int fyi = face_y_index(L, c, k);
-    const double dc = on ? L.diag[c] : 0.0;
-    const double fxl = on ? L.fx[fxi] : 0.0;
-    const double fxh = on ? L.fx[fxi + 1] : 0.0;
-    const double fyl = on ? L.fy[fyi] : 0.0;
-    const double fyh = on ? L.fy[fyi + nx] : 0.0;
-    const double fz_hi = on ? L.fz[c + plane] : 0.0;
+    const double x_next = (on && k + 1 < nz) ? x[c + plane] : 0.0;
     tile[buf][ty + 1][tx + 1] = x_cur;
     if (ring_w) tile[buf][ty + 1][tx] = x[c - 1];
     if (ring_e) tile[buf][ty + 1][tx + 2] = x[c + 1];
@@ -691,11 +680,14 @@ __global__ void __launch_bounds__(kTileX * kTileY)
       const double yp = j + 1 < ny ? tile[buf][ty + 2][tx + 1] : ((nb & 8u) ? xc : 0.0);
       const double zm = k > 0 ? x_prev : ((nb & 16u) ? xc : 0.0);
       const double zp = k + 1 < nz ? x_next : ((nb & 32u) ? xc : 0.0);
-      double v = dc * xc;
-      v -= fxl * xm;
-      v -= fxh * xp;
-      v -= fyl * ym;
-      v -= fyh * yp;
+      const int fxi = face_x_index(L, c, j, k);
+      const int fyi = face_y_index(L, c, k);
+      const double fz_hi = L.fz[c + plane];
+      double v = L.diag[c] * xc;
+      v -= L.fx[fxi] * xm;
+      v -= L.fx[fxi + 1] * xp;
+      v -= L.fy[fyi] * ym;
+      v -= L.fy[fyi + nx] * yp;
       v -= fz_lo * zm;
       v -= fz_hi * zp;
       y[c] = v;
@@ -704,7 +696,6 @@ __global__ void __launch_bounds__(kTileX * kTileY)
     }
     x_prev = x_cur;
     x_cur = x_next;
-    x_next = x_after;
     buf ^= 1;
   }
   if (finish_reduction<1>(acc, red) && threadIdx.x == 0)
