@@ -618,7 +618,7 @@ __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
 }
 
 // The Krylov operator y = A x with x.y over 3-D tiles: a CTA of kTileX x
-// kTileY threads owns those columns of (i, j) and marches up kTileZ planes.
+// kTileY threads owns those columns of (i, j) and marches up DEPTH planes.
 // Each plane of x is read from HBM once: the thread keeps its column's
 // x(k-1), x(k), x(k+1) in registers and publishes x(k) in a shared-memory
 // tile with a one-cell ring, from which the four in-plane neighbours are
@@ -629,11 +629,11 @@ __global__ void k_residual_norm(Level<double> L, const double* __restrict__ x,
 // k_residual_norm at 256^3, 0.208 against 0.180 ms, and is not used.)
 constexpr int kTileX = 32;
 constexpr int kTileY = 8;
-constexpr int kTileZ = 32;
 // Tiles per launch: at most one reduction partial each in the solver's
 // partials block (kBasisChunk * 148 * 8 doubles and more).
 constexpr long long kMaxTiledBlocks = 16384;
 
+template <int DEPTH>  // planes a CTA marches (a compile-time trip count)
 __global__ void __launch_bounds__(kTileX * kTileY)
     k_stencil_tiled(Level<double> L, const double* __restrict__ x, double* __restrict__ y,
                     Reduce red) {
@@ -648,7 +648,7 @@ __global__ void __launch_bounds__(kTileX * kTileY)
   const int bz = rest / tiles_y;
   const int tx = threadIdx.x % kTileX, ty = threadIdx.x / kTileX;
   const int i = bx * kTileX + tx, j = by * kTileY + ty;
-  const int k0 = bz * kTileZ, k1 = min(nz, k0 + kTileZ);
+  const int k0 = bz * DEPTH, k1 = min(nz, k0 + DEPTH);
   const bool on = i < nx && j < ny;
   const int ic = min(i, nx - 1), jc = min(j, ny - 1);
   const int plane = nx * ny;
@@ -1634,20 +1634,37 @@ void launch_mg_projection(cudaStream_t s, int n, const double* r,
 
 // The tiled operator serves grids whose tile count fits the reduction
 // partials.
-bool tiles_fit(const Level<double>& L) {
-  const long long tiles = static_cast<long long>((L.nx + kTileX - 1) / kTileX) *
-                          ((L.ny + kTileY - 1) / kTileY) * ((L.nz + kTileZ - 1) / kTileZ);
-  return tiles <= kMaxTiledBlocks;
+long long tile_count(const Level<double>& L, int depth) {
+  return static_cast<long long>((L.nx + kTileX - 1) / kTileX) *
+         ((L.ny + kTileY - 1) / kTileY) * ((L.nz + depth - 1) / depth);
 }
-int tiled_blocks(const Level<double>& L) {
-  return ((L.nx + kTileX - 1) / kTileX) * ((L.ny + kTileY - 1) / kTileY) *
-         ((L.nz + kTileZ - 1) / kTileZ);
+// Planes per tile: the deepest of 64, 32, 16, 8 that still gives at least
+// three quarters of a wave of resident tiles (8 per SM), so that mid-size
+// grids run in about one full wave and small ones are not left to a few SMs.
+int tile_depth(const Level<double>& L) {
+  static const int wave = [] {
+    int device = 0, sms = 0;
+    cudaGetDevice(&device);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    return 8 * (sms > 0 ? sms : 148);
+  }();
+  int depth = 64;
+  while (depth > 8 && 4 * tile_count(L, depth) < 3LL * wave) depth >>= 1;
+  return depth;
 }
 
 void launch_spmv_dot(cudaStream_t s, const Level<double>& L, const double* x,
                      double* y, Reduce red, bool tiled) {
-  if (tiled && tiles_fit(L)) {
-    launch(k_stencil_tiled, tiled_blocks(L), kTileX * kTileY, 0, s, L, x, y, red);
+  const int depth = tile_depth(L);
+  const long long tiles = tile_count(L, depth);
+  if (tiled && tiles <= kMaxTiledBlocks) {
+    const int blocks = static_cast<int>(tiles);
+    switch (depth) {
+      case 64: launch(k_stencil_tiled<64>, blocks, kTileX * kTileY, 0, s, L, x, y, red); break;
+      case 32: launch(k_stencil_tiled<32>, blocks, kTileX * kTileY, 0, s, L, x, y, red); break;
+      case 16: launch(k_stencil_tiled<16>, blocks, kTileX * kTileY, 0, s, L, x, y, red); break;
+      default: launch(k_stencil_tiled<8>, blocks, kTileX * kTileY, 0, s, L, x, y, red); break;
+    }
     return;
   }
   launch(k_spmv_dot, reduction_blocks(HFPS_CELLS(L)), kThreads, 0, s, L, x, y, red);
