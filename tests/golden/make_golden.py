@@ -7,6 +7,8 @@ Run in a tree where the reference sources are present:
     python tests/golden/make_golden.py --steps                          # assembly steps
     python tests/golden/make_golden.py --c2                             # 512x256x256
     python tests/golden/make_golden.py --null-space                     # MgNullSpace::constant
+    python tests/golden/make_golden.py --cold64                         # cold path at 64^3
+    python tests/golden/make_golden.py --cold64-spread                  # its BiCGSTAB ulp spread
 
 For each small case the script builds the seeded system with
 hfps.workloads, then records what the reference's own code returns for it
@@ -330,7 +332,125 @@ def null_space_main():
         json.dump(index, f, indent=1)
 
 
+def cold64_main():
+    """The reference's cold path on the 64^3 spherical flame: one ColdPressureIccg
+    application of the probe vector, solve_pcg + ColdPressureIccg and
+    solve_bicgstab + ColdPressureDilu at rtol 1e-12 from x0 = 0, recorded on the
+    seeded sample of cells (scale_sample) with the iteration counts."""
+    spec = dict(config="sphere64")
+    system = system_for(spec)
+    cells = scale_sample(system.cells)
+    v = probe_vector(system)
+    arrays = {"cells": cells}
+    index = {"spec": spec, "digest": input_digest(system), "sample_cells": int(cells.size)}
+    for algorithm, pc in (("pcg", "iccg"), ("bicgstab", "dilu")):
+        ref = ref_oracle.RefSession(system, ref_oracle.MgPolicy(), algorithm=algorithm,
+                                    preconditioner=pc)
+        if pc == "iccg":
+            arrays["iccg_apply"] = ref.apply_cold(v).reshape(-1)[cells]
+        x, info = ref.solve(system.rhs, rtol=1e-12, maxit=8000)
+        ref.close()
+        arrays[f"{algorithm}_{pc}_x"] = x.reshape(-1)[cells]
+        index[f"{algorithm}_{pc}"] = {"iterations": info["iterations"],
+                                      "termination": info["termination"],
+                                      "x_norm": float(np.linalg.norm(x))}
+        print(algorithm, pc, index[f"{algorithm}_{pc}"])
+    np.savez_compressed(os.path.join(HERE, "cold_path_64.npz"), **arrays)
+    with open(os.path.join(HERE, "cold_path_64.json"), "w") as f:
+        json.dump(index, f, indent=1)
+
+
+def _bicgstab_ulp_iterations(seed: int, rtol: float = 1e-12, maxit: int = 8000) -> int:
+    """solve_bicgstab + DILU on the 64^3 spherical flame in the C restatement's
+    control flow (oracle/hfps_oracle.c hfo_solve_bicgstab: early exit on |s|,
+    a true residual and a fresh start every 4 iterations), with the operator's
+    result moved by at most one ulp per cell, the move drawn from `seed`
+    (seed 0: no move, the restatement itself).  Dots are exactly rounded."""
+    import math
+    import c_oracle
+    system = system_for(dict(config="sphere64"))
+    o = c_oracle.OracleSession(system, preconditioner="dic")
+    rng = np.random.default_rng(seed)
+
+    def op(v):
+        y = o.apply_operator(v)
+        return y if seed == 0 else y + np.spacing(y) * rng.integers(-1, 2, size=y.shape)
+
+    pc = o.apply_preconditioner
+
+    def dot(a, b):
+        return math.fsum((a * b).reshape(-1))
+
+    b = system.rhs
+    x = np.zeros_like(b)
+    tol = rtol * math.sqrt(dot(b, b))
+    r = b - op(x)
+    rh = r.copy()
+    rho_prev = alpha = omega = 1.0
+    fresh, it = True, 0
+    p = v = None
+    while it < maxit:
+        rho = dot(rh, r)
+        p = r.copy() if fresh else r + ((rho / rho_prev) * (alpha / omega)) * (p - omega * v)
+        ph = pc(p)
+        v = op(ph)
+        alpha = rho / dot(rh, v)
+        s = r - alpha * v
+        if math.sqrt(dot(s, s)) <= tol:
+            x = x + alpha * ph
+            it += 1
+        else:
+            sh = pc(s)
+            t = op(sh)
+            omega = dot(t, s) / dot(t, t)
+            x = (x + alpha * ph) + omega * sh
+            r = s - omega * t
+            it += 1
+            if not (math.sqrt(dot(r, r)) <= tol or it % 4 == 0):
+                rho_prev, fresh = rho, False
+                continue
+        r = b - op(x)
+        if math.sqrt(dot(r, r)) <= tol:
+            break
+        rh = r.copy()
+        rho_prev = alpha = omega = 1.0
+        fresh = True
+    o.close()
+    return it
+
+
+def cold64_spread_main(seeds=16):
+    """How far one-ulp noise in the operator moves BiCGSTAB's iteration count
+    on the 64^3 cold path: seeds 1.. of _bicgstab_ulp_iterations beside the
+    unperturbed seed 0 (which must give the reference's own count), added to
+    cold_path_64.json as bicgstab_dilu_ulp_spread.  The GPU operator differs
+    from the reference's by rounding only (the IBM couplings are masked in the
+    coefficients instead of added as a decoration pass), so this spread, not
+    the reference's single count, is what its BiCGSTAB iteration count can be
+    held to."""
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(min(8, os.cpu_count() or 1)) as pool:
+        counts = pool.map(_bicgstab_ulp_iterations, range(seeds))
+    path = os.path.join(HERE, "cold_path_64.json")
+    with open(path) as f:
+        index = json.load(f)
+    if counts[0] != index["bicgstab_dilu"]["iterations"]:
+        raise SystemExit(f"unperturbed restatement took {counts[0]} iterations, "
+                         f"the reference {index['bicgstab_dilu']['iterations']}")
+    index["bicgstab_dilu_ulp_spread"] = {"rtol": 1e-12, "seeds": list(range(1, seeds)),
+                                         "iterations": counts[1:]}
+    print("bicgstab_dilu_ulp_spread", counts)
+    with open(path, "w") as f:
+        json.dump(index, f, indent=1)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "--cold64":
+        cold64_main()
+        raise SystemExit(0)
+    if len(sys.argv) > 1 and sys.argv[1] == "--cold64-spread":
+        cold64_spread_main()
+        raise SystemExit(0)
     if len(sys.argv) > 1 and sys.argv[1] == "--null-space":
         null_space_main()
         raise SystemExit(0)

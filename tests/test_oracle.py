@@ -473,3 +473,25 @@ def test_cold_path_matches_live_reference_with_ibm():
         x2, i2 = o.solve(s.rhs, rtol=1e-9, maxit=3000, algorithm=algorithm)
         assert i1["iterations"] == i2["iterations"]
         assert np.array_equal(x1, x2)
+
+
+def test_cold_bicgstab_restatement_at_64_cubed():
+    """The C restatement's solve_bicgstab + DILU on the 64^3 spherical flame
+    takes the reference's recorded 518 iterations and lands on its solution
+    bit for bit on the seeded sample (tests/golden/cold_path_64.*), so the
+    iteration spread recorded beside it (make_golden.py --cold64-spread,
+    seed 0 of which is this run) is measured around the reference's own
+    trajectory."""
+    import json
+    import c_oracle
+    meta = json.load(open(os.path.join(golden_cases.GOLDEN, "cold_path_64.json")))
+    gold = np.load(os.path.join(golden_cases.GOLDEN, "cold_path_64.npz"))
+    s = workloads.make("sphere64")
+    assert golden_cases.digest(s) == meta["digest"]
+    o = c_oracle.OracleSession(s, preconditioner="dic")
+    x, info = o.solve(s.rhs, rtol=1e-12, maxit=8000, algorithm="bicgstab")
+    o.close()
+    assert info["iterations"] == meta["bicgstab_dilu"]["iterations"]
+    assert np.array_equal(x.reshape(-1)[gold["cells"]], gold["bicgstab_dilu_x"])
+    spread = meta["bicgstab_dilu_ulp_spread"]["iterations"]
+    assert len(spread) >= 8 and min(spread) < info["iterations"] < max(spread)
