@@ -96,11 +96,26 @@ void launch_prolongate(cudaStream_t s, const Level<T>& F, T* x,
                        const Level<T>& C, const T* cx, int coarsen_mask, int hx = 0,
                        int hxc = 0);
 // ---- zebra line relaxation (kernels_line.cu) --------------------------------
-// Line-colour passes with more lines than this run the chunked-scan solve
+// Line-colour passes with at least kLinePcrThreshold lines (kLinePcrThresholdLong
+// for lines of kLinePcrLongExtent cells or more) run the chunked-scan solve
 // (lanes across lines, warps along chunks of one line); fewer lines run PCR
-// with one CTA row per line.  Lines longer than 2048 cells are not
-// supported (kLineNone).
-constexpr long long kLinePcrThreshold = 1024;
+// with one CTA row per line.  Lines longer than 2048 cells are not supported
+// (kLineNone).  The long-line boundary is lower because PCR's factor block
+// grows with the line (2 log2(extent) + 1 arrays against the scan's two):
+// measured MG applications, 512 lines per colour on the scan against PCR,
+// 256-cell lines (32x256x32 in the 256^3 hierarchy) 2.74 against 2.80 ms,
+// 128-cell lines (32x128x32 in the 128^3 one) 0.78 against 0.75 ms; fewer
+// than 512 lines leave most SMs idle on the scan (2.82 ms with 8x256x8 on
+// it as well).
+#ifndef HFPS_LINE_PCR_THRESHOLD
+#define HFPS_LINE_PCR_THRESHOLD 1024
+#endif
+#ifndef HFPS_LINE_PCR_THRESHOLD_LONG
+#define HFPS_LINE_PCR_THRESHOLD_LONG 512
+#endif
+constexpr long long kLinePcrThreshold = HFPS_LINE_PCR_THRESHOLD;
+constexpr long long kLinePcrThresholdLong = HFPS_LINE_PCR_THRESHOLD_LONG;
+constexpr int kLinePcrLongExtent = 256;
 enum LineKind : int { kLineNone = 0, kLineScan = 1, kLinePcr = 2 };
 int line_kind(int nx, int ny, int nz, int axis);
 // Values of the factor block of one level and line axis in precision T: the

@@ -663,7 +663,9 @@ int line_kind(int nx, int ny, int nz, int axis) {
   const int a_extent = axis == 0 ? ny : nx;
   const int b_extent = axis == 2 ? ny : nz;
   const long long per_color = static_cast<long long>((a_extent + 1) / 2) * b_extent;
-  if (per_color < kLinePcrThreshold && extent <= 1024) return kLinePcr;
+  const long long threshold =
+      extent >= kLinePcrLongExtent ? kLinePcrThresholdLong : kLinePcrThreshold;
+  if (per_color < threshold && extent <= 1024) return kLinePcr;
   return extent <= kScanMaxExtent ? kLineScan : kLineNone;
 }
 
