@@ -360,15 +360,16 @@ def cold64_main():
         json.dump(index, f, indent=1)
 
 
-def _bicgstab_ulp_iterations(seed: int, rtol: float = 1e-12, maxit: int = 8000) -> int:
-    """solve_bicgstab + DILU on the 64^3 spherical flame in the C restatement's
+def _bicgstab_ulp_iterations(seed: int, rtol: float = 1e-12, maxit: int = 8000,
+                              spec=None) -> int:
+    """solve_bicgstab + DILU on the 64^3 spherical flame (or `spec`) in the C restatement's
     control flow (oracle/hfps_oracle.c hfo_solve_bicgstab: early exit on |s|,
     a true residual and a fresh start every 4 iterations), with the operator's
     result moved by at most one ulp per cell, the move drawn from `seed`
     (seed 0: no move, the restatement itself).  Dots are exactly rounded."""
     import math
     import c_oracle
-    system = system_for(dict(config="sphere64"))
+    system = system_for(spec or dict(config="sphere64"))
     o = c_oracle.OracleSession(system, preconditioner="dic")
     rng = np.random.default_rng(seed)
 

@@ -495,3 +495,15 @@ def test_cold_bicgstab_restatement_at_64_cubed():
     assert np.array_equal(x.reshape(-1)[gold["cells"]], gold["bicgstab_dilu_x"])
     spread = meta["bicgstab_dilu_ulp_spread"]["iterations"]
     assert len(spread) >= 8 and min(spread) < info["iterations"] < max(spread)
+
+
+@pytest.mark.parametrize("name", ["sphere_24x20x16_rbV22", "wrinkled_16x40x12_lineF"])
+def test_ulp_spread_replica_follows_the_restatement(name):
+    """The Python BiCGSTAB that measures the one-ulp iteration spread
+    (make_golden.py _bicgstab_ulp_iterations) takes, unperturbed, the
+    reference's recorded iteration count on the small cold-path cases, so
+    its control flow is the restatement's (hfo_solve_bicgstab)."""
+    from golden import make_golden
+    meta = golden_cases.index()[name]
+    count = make_golden._bicgstab_ulp_iterations(0, spec=meta["spec"])
+    assert count == meta["cold"]["bicgstab_dilu"]["iterations"]
